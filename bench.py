@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the GPU runner on the 30-qubit random circuit.
+
+Workload (one step): a 30-qubit, 20-layer random circuit -- per layer a
+U3(theta, phi, lambda) on every qubit (written as U1 with its 2x2 matrix) then
+CZ (CP pi) on brick-pattern neighbour pairs -- applied to |0...0> in
+complex128 (a 16 GiB state, larger than L2), through the per-gate path.
+Metric: algorithmic HBM GB/s of the circuit (bytes each gate must read and
+write, divided by the device time of the step); ms_per_step is the circuit
+time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched under torch.distributed.run) every rank runs its own
+replica of the circuit on its own GPU: the path has no exchange step, so
+there is no collective on the data path ("replicas only").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUBITS = 30
+N_LAYERS = 20
+SEED = 2030
+METRIC = "random30_c128_circuit_hbm_gbs"
+UNIT = "GB/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--qubits", type=int, default=N_QUBITS)
+    ap.add_argument("--layers", type=int, default=N_LAYERS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def config_dict(args, world):
+    return {"workload": f"random circuit, {args.qubits} qubits, {args.layers} layers (U3 on every qubit + brick CZ), "
+                        "complex128, per-gate path",
+            "qubits": args.qubits, "layers": args.layers, "seed": SEED, "state_bytes": 16 << args.qubits,
+            "l2": "inputs larger than L2 (state >> 126 MB)", "parallelism": f"replicas x{world}"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the unmodified reference MEM runner on the host cores
+# ---------------------------------------------------------------------------
+def mem_available_bytes():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def cpu_sample(circ, n_gates):
+    from subquokka_dev_b200.engine import Circuit
+    return Circuit(circ.gate_list()[:n_gates])
+
+
+def run_cpu_baseline(circ, n, n_gates):
+    """Time the reference (oracle/_ref) or, if it was not built, the oracle's C
+    port, on the first n_gates gates of the workload.  Returns a dict."""
+    import numpy as np
+    import oracle
+    from subquokka_dev_b200.circuits import algorithmic_bytes
+    sample = cpu_sample(circ, n_gates)
+    sbytes = algorithmic_bytes(sample, n)
+    cores = os.cpu_count() or 1
+    file_qbit = max(0, int(math.floor(math.log2(cores))))
+    threads = 1 << file_qbit
+    need = (16 << n) + (2 << 30)
+    if mem_available_bytes() < need:
+        return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"skipped: host has less than {need >> 30} GiB available"}
+    desc = f"first {n_gates} gates (layer 1) of the {n}-qubit circuit, runner span only"
+    if oracle.have_reference():
+        _, secs = oracle.run_reference(n, sample.to_text(), 0, init=None, chunk_qbit=12,
+                                       file_qbit=file_qbit)
+        kind = "reference"
+    else:
+        s = np.zeros(1 << n, np.complex128)
+        s[0] = 1
+        t0 = time.perf_counter()
+        oracle.apply_circuit(s, n, sample)
+        secs = time.perf_counter() - t0
+        kind, threads = "port", cores
+    return {"value": sbytes / secs / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": desc, "seconds": secs}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from subquokka_dev_b200 import circuits
+    circ = circuits.random_u3_cz(args.qubits, args.layers, SEED)
+    n_sample = args.qubits + args.qubits // 2   # the first layer
+    for _ in range(args.warmup):
+        run_cpu_baseline(circ, args.qubits, 1)
+    vals, secs = [], []
+    cb = None
+    for _ in range(args.steps):
+        cb = run_cpu_baseline(circ, args.qubits, n_sample)
+        if cb["value"] is None:
+            print(json.dumps({"impl": "reference", "unavailable": cb["sample"]}))
+            return 0
+        vals.append(cb["value"])
+        secs.append(cb["seconds"])
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "impl": "reference", "config": config_dict(args, world),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-i", gpu_id,
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def load_traffic():
+    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return {}
+
+
+def measured_peak_hbm():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def kernel_class(g):
+    """Name of the kernel a gate launches (see csrc/qk_engine.cu launch_op)."""
+    if g.kind == 9:
+        return "k_dense1_lane" if g.q[0] < 5 else "k_dense1_pair"
+    if g.kind == 12:
+        return "k_phase2"
+    return f"kind{g.kind}"
+
+
+def our_arm(args, rank, world):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from subquokka_dev_b200 import StateVector, _lib, circuits
+    from subquokka_dev_b200._lib import check
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    n = args.qubits
+    circ = circuits.random_u3_cz(n, args.layers, SEED)
+    alg = circuits.algorithmic_bytes(circ, n)
+    S = 16 << n
+    lib = _lib.load()
+    sv = StateVector(n, "c128")
+    sv.set_stream(torch.cuda.current_stream().cuda_stream)
+    gate_ms = (ctypes.c_float * circ.ngates)()
+
+    def step(timed=False):
+        sv.reset()
+        if timed:
+            check(lib.qk_apply_gates_timed(sv.h, circ.gates, circ.ngates, gate_ms))
+        else:
+            sv.apply(circ)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        uuid = str(dev)
+    sampler = ClockSampler(uuid)
+    time.sleep(0.5)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per_kernel = {}
+    ev0.record()
+    for _ in range(args.steps):
+        step(timed=True)
+        for i, g in enumerate(circ.gate_list()):
+            per_kernel.setdefault(kernel_class(g), []).append(gate_ms[i])
+    ev1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * alg * args.steps / (total_ms / 1e3) / 1e9
+
+    # dominant kernel: the dense one-qubit sweep on a high qubit (U1, 2S bytes)
+    peak, peak_kind = measured_peak_hbm()
+    shares = {k: sum(v) for k, v in per_kernel.items()}
+    tot = sum(shares.values())
+    dom = "k_dense1_pair"
+    dom_ms = statistics.mean(per_kernel[dom])
+    achieved = 2 * S / (dom_ms / 1e3) / 1e9
+    traffic = load_traffic().get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (copy)",
+                "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
+                "avg_launch_ms": dom_ms,
+                "kernel_share": {k: v / tot for k, v in sorted(shares.items())},
+                "kernel_gbs": {k: (2 * S if k.startswith("k_dense1") else S // 2) / (statistics.mean(v) / 1e3) / 1e9
+                               for k, v in per_kernel.items()}}
+    launches = args.steps * (circ.ngates + 1)
+
+    # end to end through the public API: host gate records in, final state out to pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        try:
+            host = torch.empty(2 << n, dtype=torch.float64, pin_memory=True)
+            pinned = True
+        except Exception:
+            host = torch.empty(2 << n, dtype=torch.float64)
+            pinned = False
+        hp = ctypes.cast(host.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        e2e_steps = max(1, min(args.steps, 2))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sv.reset()
+            sv.apply(circ)
+            check(lib.qk_sv_download(sv.h, hp))
+        el = time.perf_counter() - t0
+        tt = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        el = float(tt.item())
+        import ctypes as _ct
+        e2e = {"value": world * alg * e2e_steps / el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": _ct.sizeof(circ.gates._type_) * circ.ngates,
+               "d2h_bytes_per_step": S, "ms_per_step": 1e3 * el / e2e_steps,
+               "host_buffer": "pinned" if pinned else "pageable"}
+        del host
+    sv.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_baseline(circ, n, n + n // 2)
+        cpu.pop("seconds", None)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "config": config_dict(args, world), "circuit_seconds": ms_per_step / 1e3,
+                "gates_per_s": world * circ.ngates / (ms_per_step / 1e3),
+                "hbm_frac_of_peak": value / peak,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": launches}
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        # the reference is CPU code: rank 0 alone times it, other ranks exit
+        return reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        return our_arm(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,198 @@
+/*
+ * quokka_gpu.h -- C ABI of the B200 state-vector engine (libquokka_gpu.so).
+ *
+ * The engine is a GPU runner for the SubQuokka simulator's in-memory path:
+ * the state vector of 2^N amplitudes stays resident in HBM and every gate of
+ * a circuit.txt file is applied by a hand-written sm_100a kernel.  The ABI
+ * uses plain C types only (no torch, no C++), so the reference's C++ host, a
+ * ctypes stub or any other FFI can bind it.  Every entry point returns an int
+ * status (0 = QK_OK, negative = error); the message of the last error on the
+ * calling thread is qk_last_error().  The library never exits the process.
+ *
+ * Conventions shared with the reference (src/MEM_Runner.cpp:79-81,
+ * src/MEM_Runner.cpp:90-99): amplitude k of an N-qubit state is stored at
+ * index k, qubit q is bit q of k (little-endian), each amplitude is an
+ * interleaved (re, im) pair, the initial state is |0...0>.  Multi-qubit gates
+ * take their targets in ascending order, as the reference's loop nests
+ * require; the parser refuses anything else instead of computing a wrong
+ * state.
+ *
+ * Threading: one host thread per qk_sv at a time; work is ordered on the
+ * state's CUDA stream.  Distinct handles may be used from distinct threads.
+ */
+#ifndef QUOKKA_GPU_H
+#define QUOKKA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QK_ABI_VERSION 1
+#define QK_MAX_TARGETS 12
+
+/* Status codes.  The reference reports errors by printing to cerr and calling
+ * exit(1) (src/simulator.cpp:190-193, :594-596, :764-774); here the same
+ * conditions return one of these codes. */
+typedef enum qk_status {
+    QK_OK = 0,
+    QK_ERR_ARG = -1,          /* bad argument, size or handle */
+    QK_ERR_PARSE = -2,        /* malformed circuit/ini line, unknown gate */
+    QK_ERR_QUBIT = -3,        /* target >= total qubits ("Qubit Index Error") */
+    QK_ERR_ORDER = -4,        /* multi-qubit targets not strictly ascending */
+    QK_ERR_IO = -5,           /* file could not be opened or read */
+    QK_ERR_CUDA = -6,         /* a CUDA runtime call failed */
+    QK_ERR_OOM = -7,          /* device allocation failed */
+    QK_ERR_UNSUPPORTED = -8,  /* valid input that this engine does not run */
+    QK_ERR_NOT_BUILT = -9     /* the CUDA code for this call is missing */
+} qk_status;
+
+/* Amplitude type of a state: complex128 (the reference's type) or complex64. */
+typedef enum qk_dtype { QK_C128 = 0, QK_C64 = 1 } qk_dtype;
+
+/* Gate kinds: the gate tokens of the reference's MEM parser
+ * (Simulator::setGate_MEM, src/simulator.cpp:542-597). */
+typedef enum qk_gate_kind {
+    QK_GATE_H = 1,          /* "H q"                                         */
+    QK_GATE_X = 2,          /* "X q"                                         */
+    QK_GATE_Y = 3,          /* "Y q"                                         */
+    QK_GATE_Z = 4,          /* "Z q"                                         */
+    QK_GATE_P = 5,          /* "P q phi"                                     */
+    QK_GATE_RX = 6,         /* "RX q phi"                                    */
+    QK_GATE_RY = 7,         /* "RY q phi"                                    */
+    QK_GATE_RZ = 8,         /* "RZ q phi"                                    */
+    QK_GATE_U1 = 9,         /* "U1 q" + 4 (re im) pairs, row-major 2x2       */
+    QK_GATE_U2 = 10,        /* "U2 a b" + 16 (re im) pairs, basis |a b>, a MSB */
+    QK_GATE_SWAP = 11,      /* "SWAP a b"                                    */
+    QK_GATE_CP = 12,        /* "CP a b phi"                                  */
+    QK_GATE_RZZ = 13,       /* "RZZ a b phi"                                 */
+    QK_GATE_VSWAP = 14,     /* "VSWAP_k_k" + 2k qubits: SWAP(q[i], q[k+i])  */
+    QK_GATE_MPI_VSWAP = 15  /* "MPI_VSWAP_k_k", k in {1,2}: same permutation */
+} qk_gate_kind;
+
+/* One gate as parsed from a circuit.txt line.  Angles and matrices are kept
+ * exactly as written; the engine derives the kernel coefficients on the host
+ * in FP64 with the reference's own formulas. */
+typedef struct qk_gate {
+    int32_t kind;                   /* qk_gate_kind */
+    int32_t nq;                     /* number of targets used in q[] */
+    int32_t q[QK_MAX_TARGETS];      /* targets as written */
+    double param;                   /* phi of P, RX, RY, RZ, CP, RZZ */
+    double coeff[32];               /* U1: 4, U2: 16 complex (re, im) in file order */
+} qk_gate;
+
+/* The [system] keys of the reference's .ini (setSEG/setENV,
+ * src/simulator.cpp:88-186) plus the engine's own optional keys, which the
+ * reference ignores. */
+typedef struct qk_config {
+    int32_t total_qbit;       /* total_qbit, default 0                       */
+    int32_t mpi_qbit;         /* mpi_qbit, default 0 (must be 0 here)        */
+    int32_t file_qbit;        /* file_qbit, default 0 (advisory on the GPU)  */
+    int32_t chunk_qbit;       /* chunk_qbit, default 0 (must be >= 1)        */
+    int32_t is_subcircuit;    /* is_subcircuit, default 1                    */
+    int32_t MPI_testing;      /* MPI_testing, default 0                      */
+    int32_t MPI_buffe_size;   /* MPI_buffe_size (sic), default 16            */
+    int32_t precision;        /* precision=c128|c64 -> qk_dtype, default c128 */
+    int32_t fuse_width;       /* fuse_width, default 0: per-gate kernels     */
+    int32_t dump_binary;      /* dump_format=bin -> 1, default 0 (text)      */
+    char runner_type[32];     /* runner_type, default "IO"; "GPU" selects us */
+    char dump_file[256];      /* dump_file, default ""                       */
+} qk_config;
+
+typedef struct qk_circuit qk_circuit;   /* parsed gate list (+ group sizes) */
+typedef struct qk_sv qk_sv;             /* device-resident state vector     */
+
+/* ---- errors and version ------------------------------------------------ */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *qk_last_error(void);
+/* QK_ABI_VERSION of the loaded library. */
+int qk_abi_version(void);
+
+/* ---- configuration and circuit files (host only) ----------------------- */
+
+/* Read an .ini file.  Replaces setSEG + setENV (src/simulator.cpp:88-186):
+ * same keys, same defaults, and the reference's asserts (chunk_qbit >= 1,
+ * total_qbit >= file_qbit + chunk_qbit) become QK_ERR_ARG. */
+int qk_config_load(const char *ini_path, qk_config *out);
+
+/* Parse one gate line.  Replaces Simulator::setGate_MEM and its builders
+ * (src/simulator.cpp:259-356, :542-597) and check_targ_in_N (:764-774). */
+int qk_gate_parse_line(const char *line, int total_qbit, qk_gate *out);
+
+/* Parse a whole circuit file.  is_subcircuit = 0: one gate per line
+ * (setupCircuit_MEM, src/simulator.cpp:601-615); is_subcircuit = 1: a count
+ * line followed by that many gate lines, repeated
+ * (setupSubCircuits_MEM, src/simulator.cpp:619-636). */
+int qk_circuit_load(const char *path, int is_subcircuit, int total_qbit, qk_circuit **out);
+/* Same, from an in-memory text. */
+int qk_circuit_parse(const char *text, int is_subcircuit, int total_qbit, qk_circuit **out);
+size_t qk_circuit_num_gates(const qk_circuit *c);
+const qk_gate *qk_circuit_gates(const qk_circuit *c);
+/* Number of groups and their sizes (one group per gate for flat files). */
+size_t qk_circuit_num_groups(const qk_circuit *c);
+const int32_t *qk_circuit_group_sizes(const qk_circuit *c);
+void qk_circuit_destroy(qk_circuit *c);
+
+/* Dense matrix of one gate over its targets in little-endian target order
+ * (row r, column c; bit i of r is target q[i]), FP64, built with the
+ * reference's coefficient formulas (src/circuit.cpp:2655-2991).
+ * out must hold 2 * 4^nq doubles; *dim receives 2^nq.  VSWAP gates are
+ * permutation matrices of dimension 2^(2k). */
+int qk_gate_matrix(const qk_gate *g, double *out, int *dim);
+
+/* ---- state vectors ----------------------------------------------------- */
+
+/* Allocate a 2^nqubits state on the current CUDA device and set it to
+ * |0...0>.  Replaces MEM_Runner::MEM_Runner (src/MEM_Runner.cpp:57-88). */
+int qk_sv_create(int nqubits, int dtype, qk_sv **out);
+void qk_sv_destroy(qk_sv *sv);
+/* Set |0...0>. */
+int qk_sv_reset(qk_sv *sv);
+/* Copy a host complex128 state (2^n interleaved pairs) in / out.  For a
+ * complex64 state the values are converted on the device. */
+int qk_sv_upload(qk_sv *sv, const double *host_c128);
+int qk_sv_download(qk_sv *sv, double *host_c128);
+/* Shape, type, device pointer and byte size of a state. */
+int qk_sv_info(const qk_sv *sv, int *nqubits, int *dtype, void **device_ptr, size_t *bytes);
+/* Order the state's work on a caller's cudaStream_t (NULL = default). */
+int qk_sv_set_stream(qk_sv *sv, void *cuda_stream);
+/* Wait for all work queued on the state's stream. */
+int qk_sv_synchronize(qk_sv *sv);
+
+/* ---- the hot path ------------------------------------------------------ */
+
+/* Per-gate path: apply gates[0..n) in order, one state sweep per gate.
+ * Replaces MEM_Runner::run(std::vector<Gate*>&) (src/MEM_Runner.cpp:101-134).
+ * Asynchronous on the state's stream. */
+int qk_apply_gates(qk_sv *sv, const qk_gate *gates, size_t n);
+
+/* Subcircuit path: gates are split into consecutive groups of
+ * group_sizes[0..ngroups) gates.  A group whose first gate is a VSWAP is a
+ * qubit permutation; any other group is applied in one shared-memory-resident
+ * pass over the state.  Replaces MEM_Runner::run(std::vector<std::vector<
+ * Gate*>>&) (src/MEM_Runner.cpp:136-185).  Asynchronous on the state's stream. */
+int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes, size_t ngroups);
+
+/* Per-gate path on caller-owned device memory (for example a torch tensor):
+ * state points to 2^nqubits amplitudes of dtype on the current device,
+ * cuda_stream is a cudaStream_t (NULL = default). */
+int qk_apply_gates_dev(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n,
+                       void *cuda_stream);
+
+/* Per-gate path with a CUDA event pair around every gate's kernel on the
+ * state's stream; gate_ms[i] receives gate i's device time in milliseconds.
+ * Synchronises the stream before returning.  Used for per-kernel rooflines. */
+int qk_apply_gates_timed(qk_sv *sv, const qk_gate *gates, size_t n, float *gate_ms);
+
+/* Run a parsed circuit the way Simulator::run does (src/simulator.cpp:671-706):
+ * groups if cfg->is_subcircuit, else gates; *seconds receives the device time
+ * of the runner span alone. */
+int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUOKKA_GPU_H */

@@ -1,0 +1,102 @@
+"""ORACLE -- test infrastructure only (tests/, __graft_entry__.smoke(), the
+CPU-baseline leg of bench.py).  The product never imports this package.
+
+ctypes access to the C restatement (qk_oracle.c -> liboracle.so) and to the
+unmodified reference build (_ref/quokka_ref, made by ``make -C oracle ref``
+from the reference's own sources).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+from ctypes import POINTER, c_double, c_int, c_size_t
+
+import numpy as np
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_DRIVER = os.path.join(ORACLE_DIR, "_ref", "quokka_ref")
+REF_SOURCE = "/root/reference"
+
+_lib = None
+
+
+def build(with_reference: bool | None = None) -> None:
+    """Compile the C restatement and, when the reference sources are present,
+    the reference itself (oracle/_ref)."""
+    subprocess.run(["make", "-C", ORACLE_DIR], check=True)
+    if with_reference is None:
+        with_reference = os.path.isdir(os.path.join(REF_SOURCE, "src"))
+    if with_reference:
+        subprocess.run(["make", "-C", ORACLE_DIR, "ref", "-j8", f"REF={REF_SOURCE}"], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build(with_reference=False)
+        from subquokka_dev_b200._lib import QkGate
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.qko_apply.argtypes = [POINTER(c_double), c_int, POINTER(QkGate)]
+        lib.qko_apply.restype = c_int
+        lib.qko_apply_list.argtypes = [POINTER(c_double), c_int, POINTER(QkGate), c_size_t]
+        lib.qko_apply_list.restype = c_int
+        lib.qko_expval_zz_x.argtypes = [POINTER(c_double), c_int, POINTER(c_double), POINTER(c_double)]
+        lib.qko_expval_zz_x.restype = c_double
+        _lib = lib
+    return _lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def apply_circuit(state: np.ndarray, n: int, circuit) -> np.ndarray:
+    """Apply a circuit (subquokka_dev_b200.Circuit) to a copy of state; FP64."""
+    s = np.array(state, dtype=np.complex128, copy=True)
+    rc = load().qko_apply_list(_dptr(s), n, circuit.gates, circuit.ngates)
+    if rc:
+        raise RuntimeError("oracle: unknown gate")
+    return s
+
+
+def expval_zz_x(state: np.ndarray, n: int, J, h) -> float:
+    s = np.ascontiguousarray(state, dtype=np.complex128)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    return load().qko_expval_zz_x(_dptr(s), n, _dptr(J), _dptr(h))
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_DRIVER)
+
+
+def run_reference(n: int, circuit_text: str, is_subcircuit: int, init: np.ndarray | None = None,
+                  chunk_qbit: int = 12, file_qbit: int = 0, threads: int | None = None):
+    """Run the unmodified reference MEM runner; returns (final state, runner seconds)."""
+    chunk = min(chunk_qbit, n - file_qbit)
+    with tempfile.TemporaryDirectory() as d:
+        ini = os.path.join(d, "x.ini")
+        with open(ini, "w") as f:
+            f.write(f"[system]\ntotal_qbit={n}\nfile_qbit={file_qbit}\nchunk_qbit={chunk}\n"
+                    f"runner_type=MEM\nis_subcircuit={int(is_subcircuit)}\n")
+        cir = os.path.join(d, "c.txt")
+        with open(cir, "w") as f:
+            f.write(circuit_text)
+        out = os.path.join(d, "out.bin")
+        cmd = [REF_DRIVER, "-i", ini, "-c", cir, "-o", out]
+        if init is not None:
+            ip = os.path.join(d, "init.bin")
+            np.ascontiguousarray(init, dtype=np.complex128).tofile(ip)
+            cmd += ["-s", ip]
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
+        m = re.search(r"^([0-9.eE+-]+)s$", r.stdout, re.M)
+        secs = float(m.group(1)) if m else float("nan")
+        return np.fromfile(out, dtype=np.complex128), secs

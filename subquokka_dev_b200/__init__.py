@@ -1,0 +1,14 @@
+"""B200-native state-vector engine for the SubQuokka simulator's in-memory path.
+
+The engine keeps the 2^N-amplitude state resident in HBM and applies the
+gates of the reference's circuit.txt format with hand-written sm_100a
+kernels behind a C ABI (include/quokka_gpu.h, libquokka_gpu.so).  This package
+is the Python side of that ABI: ctypes bindings (_lib), the runner mirror
+(engine) and the seeded workloads (circuits).
+"""
+from .engine import (Circuit, Config, Simulator, StateVector, apply_gates_dev, gate_line, gate_matrix,
+                     make_gate, parse_line)
+from ._lib import QkError, load as load_library
+
+__all__ = ["Circuit", "Config", "Simulator", "StateVector", "apply_gates_dev", "gate_line", "gate_matrix",
+           "make_gate", "parse_line", "QkError", "load_library"]

@@ -1,0 +1,467 @@
+// State handles, kernel dispatch and the hot-path entry points of the C ABI.
+//
+// qk_apply_gates is the GPU counterpart of MEM_Runner::run(vector<Gate*>&)
+// (src/MEM_Runner.cpp:101-134): gates in order, one state sweep each.
+// qk_apply_groups is the counterpart of MEM_Runner::run(vector<vector<Gate*>>&)
+// (src/MEM_Runner.cpp:136-185): every gate group becomes one shared-memory
+// tile pass over the state.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "qk_internal.h"
+#include "qk_kernels.cuh"
+
+using namespace qk;
+
+struct qk_sv {
+    int n = 0;
+    int dtype = QK_C128;
+    void *d = nullptr;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    Op *d_ops = nullptr;     // device copy of the tile ops of the last group call
+    size_t ops_cap = 0;
+    int device = 0;
+};
+
+namespace qk {
+
+__global__ void k_c128_to_c64(const double2 *in, float2 *out, uint64_t namp) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < namp; e += (uint64_t)gridDim.x * blockDim.x)
+        out[e] = make_float2((float)in[e].x, (float)in[e].y);
+}
+
+__global__ void k_c64_to_c128(const float2 *in, double2 *out, uint64_t namp) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < namp; e += (uint64_t)gridDim.x * blockDim.x)
+        out[e] = make_double2((double)in[e].x, (double)in[e].y);
+}
+
+static int cuda_fail(cudaError_t e, const char *what) {
+    return fail(e == cudaErrorMemoryAllocation ? QK_ERR_OOM : QK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define QK_CUDA(call)                                   \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+static int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+static unsigned sweep_blocks(uint64_t items) {
+    return (unsigned)std::max<uint64_t>(1, (items + kBlock * kUnroll - 1) / (kBlock * kUnroll));
+}
+
+// ---- tile passes ------------------------------------------------------------
+
+template <typename C> constexpr int tile_default_bits() { return sizeof(C) == 16 ? 12 : 13; }  // 64 KiB
+template <typename C> constexpr int tile_max_bits() { return sizeof(C) == 16 ? 13 : 14; }      // 128 KiB
+
+// Choose tile bits: the given qubits, the low bits 0..4 (512-byte runs for
+// complex128), then further low bits until the default tile size is reached.
+// Returns false when the qubits do not fit in one tile.
+template <typename C>
+static bool build_tile(int n, const std::vector<int> &qubits, TileDesc &d, int *local_of) {
+    std::vector<char> in(n, 0);
+    int cnt = 0;
+    for (int q : qubits)
+        if (!in[q]) { in[q] = 1; ++cnt; }
+    for (int q = 0; q < std::min(n, 5); ++q)
+        if (!in[q]) { in[q] = 1; ++cnt; }
+    const int want = std::min(n, tile_default_bits<C>());
+    for (int q = 0; q < n && cnt < want; ++q)
+        if (!in[q]) { in[q] = 1; ++cnt; }
+    if (cnt > tile_max_bits<C>()) return false;
+    std::memset(&d, 0, sizeof d);
+    d.nbits = n;
+    int k = 0;
+    for (int q = 0; q < n; ++q)
+        if (in[q]) { local_of[q] = k; d.bpos[k++] = q; }
+    d.T = k;
+    d.L = 0;
+    while (d.L < k && d.bpos[d.L] == d.L) ++d.L;
+    return true;
+}
+
+template <typename C>
+static int launch_tile(C *s, int n, const TileDesc &d, const Op *d_ops, int nops, cudaStream_t st) {
+    static bool attr_set = false;
+    const size_t smem = sizeof(C) << d.T;
+    if (!attr_set) {
+        QK_CUDA(cudaFuncSetAttribute(k_tile<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(C) << tile_max_bits<C>())));
+        attr_set = true;
+    }
+    const uint64_t ntiles = 1ull << (n - d.T);
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)num_sms() * 4);
+    k_tile<C><<<grid, kTileThreads, smem, st>>>(s, ntiles, d, d_ops, nops);
+    QK_CUDA(cudaGetLastError());
+    return QK_OK;
+}
+
+// Flat permutation sweep, used only when a VSWAP's qubits do not fit in a tile.
+template <typename C>
+__global__ void k_perm_flat(C *__restrict__ s, uint64_t namp, int k, TileDesc pairs) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < namp; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t f = e;
+        for (int i = 0; i < k; ++i) {
+            const uint64_t a = (e >> pairs.perm_a[i]) & 1, b = (e >> pairs.perm_b[i]) & 1;
+            f = (f & ~(1ull << pairs.perm_a[i]) & ~(1ull << pairs.perm_b[i])) | (b << pairs.perm_a[i]) |
+                (a << pairs.perm_b[i]);
+        }
+        if (e < f) {
+            const C a = s[e];
+            s[e] = s[f];
+            s[f] = a;
+        }
+    }
+}
+
+// ---- per-gate dispatch ------------------------------------------------------
+
+template <typename C>
+static int launch_op(C *s, int n, const Op &op, cudaStream_t st) {
+    const uint64_t namp = 1ull << n;
+    switch (op.kind) {
+    case OP_DENSE1: {
+        Mat2<C> m;
+        for (int k = 0; k < 4; ++k) m.m[k] = mk<C>(op.m[2 * k], op.m[2 * k + 1]);
+        const int t = op.q[0];
+        if (t < 5) k_dense1_lane<C><<<sweep_blocks(namp), kBlock, 0, st>>>(s, namp, t, m);
+        else k_dense1_pair<C><<<sweep_blocks(namp / 2), kBlock, 0, st>>>(s, namp / 2, t, m);
+        break;
+    }
+    case OP_PHASE1:
+        k_phase1<C><<<sweep_blocks(namp / 2), kBlock, 0, st>>>(s, namp / 2, op.q[0], mk<C>(op.m[0], op.m[1]));
+        break;
+    case OP_DIAG1:
+        k_diag1<C><<<sweep_blocks(namp), kBlock, 0, st>>>(s, namp, op.q[0], mk<C>(op.m[0], op.m[1]),
+                                                          mk<C>(op.m[2], op.m[3]));
+        break;
+    case OP_DENSE2: {
+        Mat4<C> m;
+        for (int k = 0; k < 16; ++k) m.m[k] = mk<C>(op.m[2 * k], op.m[2 * k + 1]);
+        k_dense2<C><<<sweep_blocks(namp / 4), kBlock, 0, st>>>(s, namp / 4, op.q[0], op.q[1], m);
+        break;
+    }
+    case OP_PHASE2:
+        k_phase2<C><<<sweep_blocks(namp / 4), kBlock, 0, st>>>(s, namp / 4, op.q[0], op.q[1],
+                                                               mk<C>(op.m[0], op.m[1]));
+        break;
+    case OP_DIAG2: {
+        Diag4<C> d;
+        for (int k = 0; k < 4; ++k) d.d[k] = mk<C>(op.m[2 * k], op.m[2 * k + 1]);
+        k_diag2<C><<<sweep_blocks(namp), kBlock, 0, st>>>(s, namp, op.q[0], op.q[1], d);
+        break;
+    }
+    case OP_SWAP2: {
+        const int a = std::min(op.q[0], op.q[1]), b = std::max(op.q[0], op.q[1]);
+        k_swap2<C><<<sweep_blocks(namp / 4), kBlock, 0, st>>>(s, namp / 4, a, b);
+        break;
+    }
+    case OP_PERM: {
+        // A VSWAP is a pure permutation: stage a tile holding the swapped
+        // qubits and write it back permuted, so reads and writes stay coalesced.
+        const int k = op.nq / 2;
+        std::vector<int> qs(op.q, op.q + op.nq);
+        TileDesc d;
+        std::vector<int> local(n, -1);
+        if (build_tile<C>(n, qs, d, local.data())) {
+            d.nperm = k;
+            for (int i = 0; i < k; ++i) {
+                d.perm_a[i] = local[op.q[i]];
+                d.perm_b[i] = local[op.q[k + i]];
+            }
+            return launch_tile<C>(s, n, d, nullptr, 0, st);
+        }
+        TileDesc pairs;
+        std::memset(&pairs, 0, sizeof pairs);
+        for (int i = 0; i < k; ++i) {
+            pairs.perm_a[i] = op.q[i];
+            pairs.perm_b[i] = op.q[k + i];
+        }
+        const unsigned grid = (unsigned)std::min<uint64_t>((namp + 255) / 256, (uint64_t)num_sms() * 16);
+        k_perm_flat<C><<<grid, 256, 0, st>>>(s, namp, k, pairs);
+        break;
+    }
+    default:
+        return fail(QK_ERR_ARG, "unknown op kind %d", op.kind);
+    }
+    QK_CUDA(cudaGetLastError());
+    return QK_OK;
+}
+
+template <typename C>
+static int apply_gates_t(C *s, int n, const qk_gate *gates, size_t ng, cudaStream_t st) {
+    for (size_t i = 0; i < ng; ++i) {
+        Op op;
+        int rc = lower_gate(gates[i], op);
+        if (rc) return rc;
+        for (int k = 0; k < op.nq; ++k)
+            if (op.q[k] < 0 || op.q[k] >= n)
+                return fail(QK_ERR_QUBIT, "gate %zu: qubit %d outside a %d-qubit state", i, op.q[k], n);
+        rc = launch_op<C>(s, n, op, st);
+        if (rc) return rc;
+    }
+    return QK_OK;
+}
+
+static bool is_vswap(const qk_gate &g) { return g.kind == QK_GATE_VSWAP || g.kind == QK_GATE_MPI_VSWAP; }
+
+template <typename C>
+static int apply_groups_t(qk_sv *sv, const qk_gate *gates, const int32_t *sizes, size_t ngroups) {
+    C *s = static_cast<C *>(sv->d);
+    const int n = sv->n;
+    struct Step {
+        bool tile;
+        size_t first, count;   // gates (per-gate step)
+        TileDesc d;
+        size_t op0;            // first op in the staged list (tile step)
+        int nops;
+    };
+    std::vector<Step> steps;
+    std::vector<Op> staged;
+    size_t g0 = 0;
+    for (size_t gi = 0; gi < ngroups; ++gi) {
+        if (sizes[gi] < 0) return fail(QK_ERR_ARG, "group %zu has negative size", gi);
+        const size_t cnt = (size_t)sizes[gi];
+        if (cnt == 0) continue;
+        std::vector<int> qs;
+        std::vector<Op> ops(cnt);
+        for (size_t j = 0; j < cnt; ++j) {
+            int rc = lower_gate(gates[g0 + j], ops[j]);
+            if (rc) return rc;
+            for (int k = 0; k < ops[j].nq; ++k) {
+                if (ops[j].q[k] < 0 || ops[j].q[k] >= n)
+                    return fail(QK_ERR_QUBIT, "gate %zu: qubit %d outside a %d-qubit state", g0 + j, ops[j].q[k], n);
+                qs.push_back(ops[j].q[k]);
+            }
+        }
+        Step st{};
+        TileDesc d;
+        std::vector<int> local(n, -1);
+        if (!is_vswap(gates[g0]) && build_tile<C>(n, qs, d, local.data())) {
+            st.tile = true;
+            st.d = d;
+            st.op0 = staged.size();
+            st.nops = (int)cnt;
+            for (auto &op : ops) {
+                for (int k = 0; k < op.nq; ++k) op.q[k] = local[op.q[k]];
+                staged.push_back(op);
+            }
+        } else {
+            st.tile = false;
+            st.first = g0;
+            st.count = cnt;
+        }
+        steps.push_back(st);
+        g0 += cnt;
+    }
+    if (!staged.empty()) {
+        if (staged.size() > sv->ops_cap) {
+            if (sv->d_ops) QK_CUDA(cudaFree(sv->d_ops));
+            sv->d_ops = nullptr;
+            sv->ops_cap = 0;
+            size_t cap = std::max<size_t>(staged.size(), 256);
+            QK_CUDA(cudaMalloc(&sv->d_ops, cap * sizeof(Op)));
+            sv->ops_cap = cap;
+        }
+        QK_CUDA(cudaMemcpyAsync(sv->d_ops, staged.data(), staged.size() * sizeof(Op), cudaMemcpyHostToDevice,
+                                sv->stream));
+    }
+    for (const Step &st : steps) {
+        int rc = st.tile ? launch_tile<C>(s, n, st.d, sv->d_ops + st.op0, st.nops, sv->stream)
+                         : apply_gates_t<C>(s, n, gates + st.first, st.count, sv->stream);
+        if (rc) return rc;
+    }
+    return QK_OK;
+}
+
+}  // namespace qk
+
+// ---- C ABI --------------------------------------------------------------------
+
+extern "C" {
+
+int qk_sv_create(int nqubits, int dtype, qk_sv **out) {
+    if (!out) return fail(QK_ERR_ARG, "null argument");
+    if (nqubits < 1 || nqubits > 36) return fail(QK_ERR_ARG, "nqubits must be in [1, 36], got %d", nqubits);
+    if (dtype != QK_C128 && dtype != QK_C64) return fail(QK_ERR_ARG, "unknown dtype %d", dtype);
+    auto *sv = new qk_sv();
+    sv->n = nqubits;
+    sv->dtype = dtype;
+    sv->bytes = (dtype == QK_C128 ? sizeof(double2) : sizeof(float2)) << nqubits;
+    cudaGetDevice(&sv->device);
+    cudaError_t e = cudaMalloc(&sv->d, sv->bytes);
+    if (e != cudaSuccess) {
+        delete sv;
+        return cuda_fail(e, "cudaMalloc(state)");
+    }
+    *out = sv;
+    int rc = qk_sv_reset(sv);
+    if (rc) {
+        qk_sv_destroy(sv);
+        *out = nullptr;
+        return rc;
+    }
+    clear_error();
+    return QK_OK;
+}
+
+void qk_sv_destroy(qk_sv *sv) {
+    if (!sv) return;
+    if (sv->d) cudaFree(sv->d);
+    if (sv->d_ops) cudaFree(sv->d_ops);
+    delete sv;
+}
+
+int qk_sv_reset(qk_sv *sv) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    const uint64_t namp = 1ull << sv->n;
+    const unsigned grid = (unsigned)std::min<uint64_t>((namp + 255) / 256, (uint64_t)num_sms() * 16);
+    if (sv->dtype == QK_C128) k_zero_state<double2><<<grid, 256, 0, sv->stream>>>((double2 *)sv->d, namp);
+    else k_zero_state<float2><<<grid, 256, 0, sv->stream>>>((float2 *)sv->d, namp);
+    QK_CUDA(cudaGetLastError());
+    return QK_OK;
+}
+
+// Host complex128 <-> device state, converted in bounded chunks for c64.
+int qk_sv_upload(qk_sv *sv, const double *host) {
+    if (!sv || !host) return fail(QK_ERR_ARG, "null argument");
+    if (sv->dtype == QK_C128) {
+        QK_CUDA(cudaMemcpyAsync(sv->d, host, sv->bytes, cudaMemcpyHostToDevice, sv->stream));
+        QK_CUDA(cudaStreamSynchronize(sv->stream));
+        return QK_OK;
+    }
+    const uint64_t namp = 1ull << sv->n;
+    const uint64_t chunk = std::min<uint64_t>(namp, 1ull << 24);
+    double2 *tmp = nullptr;
+    QK_CUDA(cudaMalloc(&tmp, chunk * sizeof(double2)));
+    int rc = QK_OK;
+    for (uint64_t off = 0; off < namp && !rc; off += chunk) {
+        cudaError_t e = cudaMemcpyAsync(tmp, host + 2 * off, chunk * sizeof(double2), cudaMemcpyHostToDevice, sv->stream);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "upload"); break; }
+        k_c128_to_c64<<<(unsigned)((chunk + 255) / 256), 256, 0, sv->stream>>>(tmp, (float2 *)sv->d + off, chunk);
+    }
+    cudaError_t e = cudaStreamSynchronize(sv->stream);
+    cudaFree(tmp);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "upload");
+    return rc;
+}
+
+int qk_sv_download(qk_sv *sv, double *host) {
+    if (!sv || !host) return fail(QK_ERR_ARG, "null argument");
+    if (sv->dtype == QK_C128) {
+        QK_CUDA(cudaMemcpyAsync(host, sv->d, sv->bytes, cudaMemcpyDeviceToHost, sv->stream));
+        QK_CUDA(cudaStreamSynchronize(sv->stream));
+        return QK_OK;
+    }
+    const uint64_t namp = 1ull << sv->n;
+    const uint64_t chunk = std::min<uint64_t>(namp, 1ull << 24);
+    double2 *tmp = nullptr;
+    QK_CUDA(cudaMalloc(&tmp, chunk * sizeof(double2)));
+    int rc = QK_OK;
+    for (uint64_t off = 0; off < namp && !rc; off += chunk) {
+        k_c64_to_c128<<<(unsigned)((chunk + 255) / 256), 256, 0, sv->stream>>>((const float2 *)sv->d + off, tmp, chunk);
+        cudaError_t e = cudaMemcpyAsync(host + 2 * off, tmp, chunk * sizeof(double2), cudaMemcpyDeviceToHost, sv->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "download");
+    }
+    cudaFree(tmp);
+    return rc;
+}
+
+int qk_sv_info(const qk_sv *sv, int *nqubits, int *dtype, void **device_ptr, size_t *bytes) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    if (nqubits) *nqubits = sv->n;
+    if (dtype) *dtype = sv->dtype;
+    if (device_ptr) *device_ptr = sv->d;
+    if (bytes) *bytes = sv->bytes;
+    return QK_OK;
+}
+
+int qk_sv_set_stream(qk_sv *sv, void *stream) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    sv->stream = (cudaStream_t)stream;
+    return QK_OK;
+}
+
+int qk_sv_synchronize(qk_sv *sv) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    QK_CUDA(cudaStreamSynchronize(sv->stream));
+    return QK_OK;
+}
+
+int qk_apply_gates_dev(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n, void *stream) {
+    if (!state || (!gates && n)) return fail(QK_ERR_ARG, "null argument");
+    if (nqubits < 1 || nqubits > 36) return fail(QK_ERR_ARG, "nqubits must be in [1, 36], got %d", nqubits);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == QK_C128) return apply_gates_t<double2>((double2 *)state, nqubits, gates, n, st);
+    if (dtype == QK_C64) return apply_gates_t<float2>((float2 *)state, nqubits, gates, n, st);
+    return fail(QK_ERR_ARG, "unknown dtype %d", dtype);
+}
+
+int qk_apply_gates(qk_sv *sv, const qk_gate *gates, size_t n) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    return qk_apply_gates_dev(sv->d, sv->n, sv->dtype, gates, n, sv->stream);
+}
+
+int qk_apply_gates_timed(qk_sv *sv, const qk_gate *gates, size_t n, float *gate_ms) {
+    if (!sv || !gate_ms || (!gates && n)) return fail(QK_ERR_ARG, "null argument");
+    std::vector<cudaEvent_t> ev(n + 1);
+    for (auto &e : ev) QK_CUDA(cudaEventCreate(&e));
+    int rc = QK_OK;
+    cudaError_t ce = cudaEventRecord(ev[0], sv->stream);
+    for (size_t i = 0; i < n && !rc && ce == cudaSuccess; ++i) {
+        rc = qk_apply_gates_dev(sv->d, sv->n, sv->dtype, gates + i, 1, sv->stream);
+        if (!rc) ce = cudaEventRecord(ev[i + 1], sv->stream);
+    }
+    if (!rc && ce == cudaSuccess) ce = cudaEventSynchronize(ev[n]);
+    for (size_t i = 0; i < n && !rc && ce == cudaSuccess; ++i) ce = cudaEventElapsedTime(&gate_ms[i], ev[i], ev[i + 1]);
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (!rc && ce != cudaSuccess) rc = cuda_fail(ce, "per-gate timing");
+    return rc;
+}
+
+int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes, size_t ngroups) {
+    if (!sv || (!group_sizes && ngroups)) return fail(QK_ERR_ARG, "null argument");
+    if (sv->dtype == QK_C128) return apply_groups_t<double2>(sv, gates, group_sizes, ngroups);
+    return apply_groups_t<float2>(sv, gates, group_sizes, ngroups);
+}
+
+int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds) {
+    if (!cfg || !c || !sv) return fail(QK_ERR_ARG, "null argument");
+    cudaEvent_t t0, t1;
+    QK_CUDA(cudaEventCreate(&t0));
+    QK_CUDA(cudaEventCreate(&t1));
+    QK_CUDA(cudaEventRecord(t0, sv->stream));
+    int rc = cfg->is_subcircuit
+                 ? qk_apply_groups(sv, c->gates.data(), c->group_sizes.data(), c->group_sizes.size())
+                 : qk_apply_gates(sv, c->gates.data(), c->gates.size());
+    if (!rc) {
+        cudaError_t e = cudaEventRecord(t1, sv->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+        if (e != cudaSuccess) rc = cuda_fail(e, "timing");
+        else if (seconds) *seconds = ms / 1e3;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+"""Host-side mirror of the reference's runner interface over the C ABI.
+
+``Simulator(ini, cir).run()`` mirrors the reference's ``Simulator`` class
+(src/simulator.hpp:51-83, src/simulator.cpp:671-724): it reads the same .ini
+and circuit.txt files, runs the circuit on the GPU runner and reports the
+runner-only time.  ``StateVector`` is the device-resident state that replaces
+``MEM_Runner::buffer`` (src/MEM_Runner.hpp:27).  Every call goes through
+libquokka_gpu.so; nothing here computes amplitudes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, byref, c_double, c_int, c_int32, c_size_t, c_void_p
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import GATE_KINDS, KIND_NAMES, QK_C64, QK_C128, QkConfig, QkGate, check
+
+DTYPES = {"c128": QK_C128, "c64": QK_C64, QK_C128: QK_C128, QK_C64: QK_C64}
+
+
+# ---------------------------------------------------------------------------
+# gates and circuits
+# ---------------------------------------------------------------------------
+def make_gate(name: str, qubits: Sequence[int], param: float = 0.0, coeff=None) -> QkGate:
+    """Build one gate record (the struct qk_gate of include/quokka_gpu.h)."""
+    g = QkGate()
+    g.kind = GATE_KINDS[name]
+    g.nq = len(qubits)
+    for i, q in enumerate(qubits):
+        g.q[i] = int(q)
+    g.param = float(param)
+    if coeff is not None:
+        flat = []
+        for z in np.asarray(coeff, dtype=np.complex128).ravel():
+            flat += [float(z.real), float(z.imag)]
+        for i, v in enumerate(flat):
+            g.coeff[i] = v
+    return g
+
+
+def gate_line(g: QkGate) -> str:
+    """circuit.txt line of a gate, with round-trip exact floats."""
+    name = KIND_NAMES[g.kind]
+    qs = [g.q[i] for i in range(g.nq)]
+    if name in ("VSWAP", "MPI_VSWAP"):
+        k = g.nq // 2
+        name = f"{name}_{k}_{k}"
+    parts = [name] + [str(q) for q in qs]
+    if name in ("P", "RX", "RY", "RZ", "CP", "RZZ"):
+        parts.append(repr(float(g.param)))
+    ncoef = {"U1": 4, "U2": 16}.get(name, 0)
+    parts += [repr(float(g.coeff[i])) for i in range(2 * ncoef)]
+    return " ".join(parts)
+
+
+class Circuit:
+    """A parsed gate list plus group sizes (one group per gate for flat files)."""
+
+    def __init__(self, gates: Iterable[QkGate], group_sizes: Sequence[int] | None = None):
+        gl = list(gates)
+        self.gates = (QkGate * max(1, len(gl)))(*gl)
+        self.ngates = len(gl)
+        gs = list(group_sizes) if group_sizes is not None else [1] * len(gl)
+        if sum(gs) != len(gl):
+            raise ValueError("group sizes do not add up to the gate count")
+        self.group_sizes = (c_int32 * max(1, len(gs)))(*gs)
+        self.ngroups = len(gs)
+
+    @classmethod
+    def _from_handle(cls, h: c_void_p) -> "Circuit":
+        lib = _lib.load()
+        try:
+            ng = lib.qk_circuit_num_gates(h)
+            gp = lib.qk_circuit_gates(h)
+            gates = [QkGate.from_buffer_copy(gp[i]) for i in range(ng)]
+            nG = lib.qk_circuit_num_groups(h)
+            sp = lib.qk_circuit_group_sizes(h)
+            sizes = [sp[i] for i in range(nG)]
+        finally:
+            lib.qk_circuit_destroy(h)
+        return cls(gates, sizes)
+
+    @classmethod
+    def load(cls, path: str, is_subcircuit: int, total_qbit: int) -> "Circuit":
+        h = c_void_p()
+        check(_lib.load().qk_circuit_load(path.encode(), int(is_subcircuit), int(total_qbit), byref(h)))
+        return cls._from_handle(h)
+
+    @classmethod
+    def parse(cls, text: str, is_subcircuit: int, total_qbit: int) -> "Circuit":
+        h = c_void_p()
+        check(_lib.load().qk_circuit_parse(text.encode(), int(is_subcircuit), int(total_qbit), byref(h)))
+        return cls._from_handle(h)
+
+    def gate_list(self) -> list[QkGate]:
+        return [self.gates[i] for i in range(self.ngates)]
+
+    def to_text(self, is_subcircuit: bool = False) -> str:
+        lines = []
+        if not is_subcircuit:
+            lines = [gate_line(self.gates[i]) for i in range(self.ngates)]
+        else:
+            k = 0
+            for gi in range(self.ngroups):
+                n = self.group_sizes[gi]
+                lines.append(str(n))
+                lines += [gate_line(self.gates[k + j]) for j in range(n)]
+                k += n
+        return "\n".join(lines) + "\n"
+
+
+def parse_line(line: str, total_qbit: int) -> QkGate:
+    g = QkGate()
+    check(_lib.load().qk_gate_parse_line(line.encode(), int(total_qbit), byref(g)))
+    return g
+
+
+def gate_matrix(g: QkGate) -> np.ndarray:
+    """Dense FP64 matrix of a gate over its targets (little-endian target order)."""
+    dim = 1 << g.nq
+    out = (c_double * (2 * dim * dim))()
+    d = c_int()
+    check(_lib.load().qk_gate_matrix(byref(g), out, byref(d)))
+    a = np.frombuffer(out, dtype=np.float64).copy().view(np.complex128)
+    return a.reshape(dim, dim)
+
+
+# ---------------------------------------------------------------------------
+# configuration
+# ---------------------------------------------------------------------------
+class Config:
+    """The [system] section of an .ini file (setSEG/setENV keys + engine keys)."""
+
+    def __init__(self, path: str):
+        self.raw = QkConfig()
+        check(_lib.load().qk_config_load(path.encode(), byref(self.raw)))
+
+    def __getattr__(self, name):
+        raw = object.__getattribute__(self, "raw")
+        v = getattr(raw, name)
+        return v.decode() if isinstance(v, bytes) else v
+
+
+# ---------------------------------------------------------------------------
+# device state
+# ---------------------------------------------------------------------------
+class StateVector:
+    """A 2^n-amplitude state resident in HBM (complex128 or complex64)."""
+
+    def __init__(self, nqubits: int, dtype="c128"):
+        self._lib = _lib.load()
+        self.h = c_void_p()
+        check(self._lib.qk_sv_create(int(nqubits), DTYPES[dtype], byref(self.h)))
+        self.nqubits = int(nqubits)
+        self.dtype = DTYPES[dtype]
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.qk_sv_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def namp(self) -> int:
+        return 1 << self.nqubits
+
+    def info(self):
+        n, dt, p, b = c_int(), c_int(), c_void_p(), c_size_t()
+        check(self._lib.qk_sv_info(self.h, byref(n), byref(dt), byref(p), byref(b)))
+        return n.value, dt.value, p.value, b.value
+
+    @property
+    def device_ptr(self) -> int:
+        return self.info()[2]
+
+    @property
+    def nbytes(self) -> int:
+        return self.info()[3]
+
+    def reset(self) -> None:
+        check(self._lib.qk_sv_reset(self.h))
+
+    def upload(self, state: np.ndarray) -> None:
+        a = np.ascontiguousarray(state, dtype=np.complex128)
+        if a.size != self.namp:
+            raise ValueError(f"state has {a.size} amplitudes, expected {self.namp}")
+        check(self._lib.qk_sv_upload(self.h, a.ctypes.data_as(POINTER(c_double))))
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.namp, dtype=np.complex128)
+        check(self._lib.qk_sv_download(self.h, out.ctypes.data_as(POINTER(c_double))))
+        return out
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(self._lib.qk_sv_set_stream(self.h, c_void_p(stream_ptr or 0)))
+
+    def synchronize(self) -> None:
+        check(self._lib.qk_sv_synchronize(self.h))
+
+    def apply(self, circuit: Circuit) -> None:
+        """Per-gate path (MEM_Runner::run(vector<Gate*>&))."""
+        check(self._lib.qk_apply_gates(self.h, circuit.gates, circuit.ngates))
+
+    def apply_groups(self, circuit: Circuit) -> None:
+        """Subcircuit path (MEM_Runner::run(vector<vector<Gate*>>&))."""
+        check(self._lib.qk_apply_groups(self.h, circuit.gates, circuit.group_sizes, circuit.ngroups))
+
+
+def apply_gates_dev(ptr: int, nqubits: int, dtype, circuit: Circuit, stream_ptr: int | None = None) -> None:
+    """Per-gate path on caller-owned device memory (e.g. a torch tensor)."""
+    check(_lib.load().qk_apply_gates_dev(c_void_p(ptr), int(nqubits), DTYPES[dtype], circuit.gates,
+                                         circuit.ngates, c_void_p(stream_ptr or 0)))
+
+
+# ---------------------------------------------------------------------------
+# the reference-facing runner
+# ---------------------------------------------------------------------------
+class Simulator:
+    """``Simulator(ini, cir)`` + ``run()`` with runner_type=GPU.
+
+    Mirrors src/simulator.cpp:708-724 (construction: read ini, parse circuit,
+    allocate the |0...0> state) and :671-706 (run: time the runner span only).
+    """
+
+    def __init__(self, ini: str, cir: str):
+        self.config = Config(ini)
+        if self.config.runner_type not in ("GPU", "MEM"):
+            raise _lib.QkError(-1, f"[Config File]: {self.config.runner_type} runner not found.")
+        if self.config.mpi_qbit:
+            raise _lib.QkError(-8, "mpi_qbit > 0 is not supported by the GPU runner")
+        self.circuit = Circuit.load(cir, self.config.is_subcircuit, self.config.total_qbit)
+        self.state = StateVector(self.config.total_qbit, self.config.precision)
+
+    def run(self) -> float:
+        sec = c_double()
+        h = c_void_p()
+        lib = _lib.load()
+        # qk_run takes the parsed circuit handle; rebuild one from our records
+        text = self.circuit.to_text(bool(self.config.is_subcircuit))
+        check(lib.qk_circuit_parse(text.encode(), self.config.is_subcircuit, self.config.total_qbit, byref(h)))
+        try:
+            check(lib.qk_run(byref(self.config.raw), h, self.state.h, byref(sec)))
+        finally:
+            lib.qk_circuit_destroy(h)
+        return sec.value

@@ -1,0 +1,201 @@
+"""Parity of the CUDA path with the reference (golden states) and the oracle.
+
+Bar: complex128 max |delta amp| <= 1e-12 against the reference's complex128
+state; complex64 within 2e-6 (FP32 rounding of the stored state).  Every test
+calls the engine through the C ABI (libquokka_gpu.so)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from subquokka_dev_b200 import Circuit, StateVector, apply_gates_dev, circuits, make_gate
+
+import golden_util as gu
+
+pytestmark = pytest.mark.gpu
+
+TOL_C128 = 1e-12
+TOL_C64 = 2e-6
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "subquokka_dev_b200", "bin", "quokka")
+
+
+def run_gpu(n, circ, init, dtype="c128", groups=False):
+    with StateVector(n, dtype) as sv:
+        if init is not None:
+            sv.upload(init)
+        if groups:
+            sv.apply_groups(circ)
+        else:
+            sv.apply(circ)
+        return sv.download()
+
+
+@pytest.mark.parametrize("name", gu.names())
+def test_per_gate_path_matches_reference(name):
+    rec = gu.load(name)
+    circ = Circuit.parse(rec["circuit"], rec["is_subcircuit"], rec["n"])
+    out = run_gpu(rec["n"], circ, gu.initial_state(rec))
+    assert gu.compare(rec, out) <= TOL_C128
+
+
+@pytest.mark.parametrize("name", gu.names())
+def test_group_path_matches_reference(name):
+    # flat fixtures run as one group per gate: every op kind goes through the tile pass
+    rec = gu.load(name)
+    circ = Circuit.parse(rec["circuit"], rec["is_subcircuit"], rec["n"])
+    out = run_gpu(rec["n"], circ, gu.initial_state(rec), groups=True)
+    assert gu.compare(rec, out) <= TOL_C128
+
+
+@pytest.mark.parametrize("name", gu.names())
+def test_c64_path_matches_reference(name):
+    rec = gu.load(name)
+    circ = Circuit.parse(rec["circuit"], rec["is_subcircuit"], rec["n"])
+    init = gu.initial_state(rec)
+    assert gu.compare(rec, run_gpu(rec["n"], circ, init, "c64")) <= TOL_C64
+    assert gu.compare(rec, run_gpu(rec["n"], circ, init, "c64", groups=True)) <= TOL_C64
+
+
+def random_gate(rng, kind, qs):
+    if kind in ("P", "RX", "RY", "RZ", "CP", "RZZ"):
+        return make_gate(kind, qs, rng.uniform(-7, 7))
+    if kind in ("U1", "U2"):
+        d = 2 if kind == "U1" else 4
+        z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+        q, _ = np.linalg.qr(z)
+        return make_gate(kind, qs, coeff=q)
+    return make_gate(kind, qs)
+
+
+@pytest.mark.parametrize("kind", ["H", "X", "Y", "Z", "P", "RX", "RY", "RZ", "U1"])
+def test_one_qubit_gate_on_every_qubit(kind):
+    n = 13
+    rng = np.random.default_rng(sum(map(ord, kind)))
+    init = circuits.random_state(n, 7)
+    for q in range(n):
+        circ = Circuit([random_gate(rng, kind, [q])])
+        ref = oracle.apply_circuit(init, n, circ)
+        assert np.abs(run_gpu(n, circ, init) - ref).max() <= TOL_C128, q
+        assert np.abs(run_gpu(n, circ, init, groups=True) - ref).max() <= TOL_C128, q
+
+
+@pytest.mark.parametrize("kind", ["U2", "SWAP", "CP", "RZZ"])
+def test_two_qubit_gate_on_many_pairs(kind):
+    n = 13
+    rng = np.random.default_rng(sum(map(ord, kind)))
+    init = circuits.random_state(n, 8)
+    pairs = [(0, 1), (0, 4), (0, 12), (3, 4), (4, 5), (4, 9), (5, 6), (5, 12), (11, 12), (1, 7)]
+    for a, b in pairs:
+        circ = Circuit([random_gate(rng, kind, [a, b])])
+        ref = oracle.apply_circuit(init, n, circ)
+        assert np.abs(run_gpu(n, circ, init) - ref).max() <= TOL_C128, (a, b)
+        assert np.abs(run_gpu(n, circ, init, groups=True) - ref).max() <= TOL_C128, (a, b)
+
+
+@pytest.mark.parametrize("qs", [
+    [0, 1, 2, 7, 8, 9], [2, 5, 9, 10, 11, 13], [0, 3, 6, 9, 12, 1, 4, 7],
+    [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13],      # VSWAP_6_6: does not fit one tile
+    [6, 7, 8, 9, 10, 11, 12, 13, 0, 1, 2, 3],
+])
+def test_vswap_k_k_intended_semantics(qs):
+    # VSWAP_k_k = SWAP(q[i], q[k+i]) for i < k (the reference's MEM versions of
+    # k >= 3 index the wrong buffer, so the oracle states the documented intent)
+    n = 14
+    init = circuits.random_state(n, 9)
+    circ = Circuit([make_gate("VSWAP", qs)])
+    ref = oracle.apply_circuit(init, n, circ)
+    k = len(qs) // 2
+    swaps = Circuit([make_gate("SWAP", sorted([qs[i], qs[k + i]])) for i in range(k)])
+    assert np.abs(oracle.apply_circuit(init, n, swaps) - ref).max() == 0
+    assert np.abs(run_gpu(n, circ, init) - ref).max() == 0
+    assert np.abs(run_gpu(n, circ, init, groups=True) - ref).max() == 0
+
+
+def test_qft20_config_matches_oracle():
+    # 20-qubit QFT on a seeded random normalised complex128 state, per-gate path
+    n = 20
+    init = circuits.random_state(n, 20)
+    circ = circuits.qft(n)
+    ref = oracle.apply_circuit(init, n, circ)
+    assert np.abs(run_gpu(n, circ, init) - ref).max() <= TOL_C128
+
+
+def test_random_circuit_family_matches_oracle():
+    n = 16
+    circ = circuits.random_u3_cz(n, 6, 30)
+    ref = oracle.apply_circuit(gu.initial_state({"n": n, "sampled": False, "init": np.zeros(0)}), n, circ)
+    assert np.abs(run_gpu(n, circ, None) - ref).max() <= TOL_C128
+    assert np.abs(run_gpu(n, circ, None, groups=True) - ref).max() <= TOL_C128
+
+
+def inverse(circ):
+    out = []
+    for g in reversed(circ.gate_list()):
+        if g.kind == 9:  # U1
+            m = np.array([g.coeff[2 * k] + 1j * g.coeff[2 * k + 1] for k in range(4)]).reshape(2, 2)
+            out.append(make_gate("U1", [g.q[0]], coeff=m.conj().T))
+        elif g.kind == 12:  # CP
+            out.append(make_gate("CP", [g.q[0], g.q[1]], -g.param))
+        else:
+            raise ValueError(g.kind)
+    return Circuit(out)
+
+
+@pytest.mark.parametrize("n,layers", [(28, 3), (31, 1)])
+def test_large_state_round_trip(n, layers):
+    # size-independent property at full scale: C then C^-1 returns |0...0>;
+    # n = 31 puts amplitude indices above 2^31
+    circ = circuits.random_u3_cz(n, layers, 31)
+    inv = inverse(circ)
+    with StateVector(n) as sv:
+        sv.apply(circ)
+        sv.apply(inv)
+        out = sv.download()
+    assert abs(out[0] - 1) < 1e-10
+    assert np.abs(out[1:]).max() < 1e-10
+
+
+def test_apply_on_caller_device_memory():
+    import torch
+    n = 12
+    circ = circuits.random_u3_cz(n, 3, 5)
+    t = torch.zeros(1 << n, dtype=torch.complex128, device="cuda")
+    t[0] = 1
+    apply_gates_dev(t.data_ptr(), n, "c128", circ, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.abs(t.cpu().numpy() - run_gpu(n, circ, None)).max() == 0
+
+
+def test_cli_dump_matches_reference_golden(tmp_path):
+    rec = gu.load("sub12")
+    ini = tmp_path / "x.ini"
+    ini.write_text(f"[system]\ntotal_qbit={rec['n']}\nfile_qbit=2\nchunk_qbit=6\nrunner_type=GPU\n"
+                   f"is_subcircuit=1\ndump_file={tmp_path}/state.bin\ndump_format=bin\n")
+    cir = tmp_path / "c.txt"
+    # the fixture starts from a random state; run the same circuit from |0> on both sides
+    cir.write_text(rec["circuit"])
+    r = subprocess.run([CLI, "-i", str(ini), "-c", str(cir)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    assert lines[0] == "GPU Mode" and lines[-1].endswith("s")
+    out = np.fromfile(tmp_path / "state.bin", dtype=np.complex128)
+    circ = Circuit.parse(rec["circuit"], 1, rec["n"])
+    z = np.zeros(1 << rec["n"], np.complex128)
+    z[0] = 1
+    assert np.abs(out - oracle.apply_circuit(z, rec["n"], circ)).max() <= TOL_C128
+
+
+def test_cli_text_dump_format(tmp_path):
+    # the reference's dump: dump_file[0:3] + rank + ".txt", "%.11f" per line
+    ini = tmp_path / "x.ini"
+    ini.write_text("[system]\ntotal_qbit=3\nfile_qbit=1\nchunk_qbit=1\nrunner_type=GPU\nis_subcircuit=0\n"
+                   "dump_file=res.txt\nMPI_testing=1\n")
+    cir = tmp_path / "c.txt"
+    cir.write_text("H 0\nH 1\nH 2\n")
+    r = subprocess.run([CLI, "-i", str(ini), "-c", str(cir)], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    vals = (tmp_path / "res0.txt").read_text().split()
+    assert len(vals) == 16 and vals[0] == "%.11f" % (0.70710678118 ** 3) and vals[1] == "0.00000000000"
