@@ -180,7 +180,8 @@ def test_cli_dump_matches_reference_golden(tmp_path):
     r = subprocess.run([CLI, "-i", str(ini), "-c", str(cir)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     lines = r.stdout.splitlines()
-    assert lines[0] == "GPU Mode" and lines[-1].endswith("s")
+    assert lines[0].startswith("[Config File]: ") and lines[1].startswith("[Circuit File]: ")
+    assert lines[2] == "GPU Mode" and lines[-1].endswith("s")
     out = np.fromfile(tmp_path / "state.bin", dtype=np.complex128)
     circ = Circuit.parse(rec["circuit"], 1, rec["n"])
     z = np.zeros(1 << rec["n"], np.complex128)
