@@ -47,6 +47,7 @@ def parse_args():
     ap.add_argument("--layers", type=int, default=N_LAYERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fused", action="store_true")
     return ap.parse_args()
 
 
@@ -203,6 +204,65 @@ def kernel_class(g):
     return f"kind{g.kind}"
 
 
+def time_device(fn, warmup, steps):
+    """Device time (ms) per call of fn, CUDA events on the current stream."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def compare_states(a, b):
+    """(max |delta amp|, 1 - fidelity) of two device states, on the GPU."""
+    import torch
+    x, y = a.as_torch(), b.as_torch()
+    chunk = 1 << 26
+    dmax, ov, nx, ny = 0.0, 0j, 0.0, 0.0
+    for i in range(0, x.numel(), chunk):
+        xs = x[i:i + chunk].to(torch.complex128)
+        ys = y[i:i + chunk].to(torch.complex128)
+        dmax = max(dmax, float((xs - ys).abs().max()))
+        ov += complex(torch.vdot(xs, ys))
+        nx += float(torch.vdot(xs, xs).real)
+        ny += float(torch.vdot(ys, ys).real)
+    return dmax, 1.0 - abs(ov) ** 2 / (nx * ny)
+
+
+def fused_variants(args, circ, exact, plain_ms, alg):
+    """The same circuit through fused passes, complex128 and complex64; each is
+    compared with the exact per-gate complex128 state left in `exact`."""
+    import torch
+    from subquokka_dev_b200 import Plan, StateVector
+    out = {}
+    n = args.qubits
+    for dtype in ("c128", "c64"):
+        plan = Plan(circ, n, dtype)
+        passes, ops, remaps = plan.stats()
+        sv = StateVector(n, dtype)
+        sv.set_stream(torch.cuda.current_stream().cuda_stream)
+
+        def run():
+            sv.reset()
+            plan.apply(sv)
+        ms = time_device(run, 2, max(1, args.steps))
+        dmax, infid = compare_states(sv, exact)
+        amp = 16 if dtype == "c128" else 8
+        out[dtype] = {"ms_per_circuit": ms, "speedup_vs_plain_c128": plain_ms / ms, "passes": passes,
+                      "program_ops": ops, "remaps": remaps,
+                      "hbm_gbs_passes": passes * 2 * (amp << n) / (ms / 1e3) / 1e9,
+                      "max_abs_damp_vs_c128": dmax, "one_minus_fidelity_vs_c128": infid}
+        sv.close()
+        plan.close()
+    return out
+
+
 def our_arm(args, rank, world):
     import numpy as np
     import torch
@@ -278,6 +338,7 @@ def our_arm(args, rank, world):
                 "kernel_gbs": {k: (2 * S if k.startswith("k_dense1") else S // 2) / (statistics.mean(v) / 1e3) / 1e9
                                for k, v in per_kernel.items()}}
     launches = args.steps * (circ.ngates + 1)
+    variants = {} if args.no_fused else fused_variants(args, circ, sv, ms_per_step, alg)
 
     # end to end through the public API: host gate records in, final state out to pinned host memory
     e2e = None
@@ -324,6 +385,7 @@ def our_arm(args, rank, world):
                 "gates_per_s": world * circ.ngates / (ms_per_step / 1e3),
                 "hbm_frac_of_peak": value / peak,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "fused": variants,
                 "gpu_launches": launches}
         print(json.dumps(line))
     return 0

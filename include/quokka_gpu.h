@@ -187,6 +187,38 @@ int qk_apply_gates_dev(void *state, int nqubits, int dtype, const qk_gate *gates
  * Synchronises the stream before returning.  Used for per-kernel rooflines. */
 int qk_apply_gates_timed(qk_sv *sv, const qk_gate *gates, size_t n, float *gate_ms);
 
+/* ---- fused passes ------------------------------------------------------ */
+
+/* Options of a fused plan; zero fields take the defaults. */
+typedef struct qk_plan_opts {
+    int32_t dtype;        /* qk_dtype of the states the plan runs on        */
+    int32_t tile_bits;    /* qubits per shared-memory tile (default 12 for
+                             complex128, 13 for complex64; at most 14)      */
+    int32_t reg_bits;     /* qubits held in registers per thread (default 3
+                             for complex128, 4 for complex64; at most 5)    */
+    int32_t reserved[5];
+} qk_plan_opts;
+
+typedef struct qk_plan qk_plan;
+
+/* Fuse a flat gate list into passes: each pass is one HBM read and write of
+ * the state that applies every gate it carries in shared memory and
+ * registers.  This replaces the reference's two-step recipe -- group gates
+ * into 12-qubit chunks with subcircuitFinder (subcircuitFinder/finder.cpp:
+ * 629-698) and run the groups chunk by chunk (src/MEM_Runner.cpp:172-183) --
+ * for any circuit, with no VSWAP: a tile's qubits need not be contiguous. */
+int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_opts *opts, qk_plan **out);
+/* One pass per group of a subcircuit file (groups that do not fit one tile
+ * are split); VSWAP groups become permutation passes. */
+int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size_t ngroups, int nqubits,
+                          const qk_plan_opts *opts, qk_plan **out);
+/* Number of passes, program operations and register re-mappings. */
+int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t *remaps);
+/* Run a plan on a state (same qubit count and dtype).  The first call copies
+ * the plan's programs to the device (owned by the plan). */
+int qk_plan_apply(qk_sv *sv, qk_plan *p);
+void qk_plan_destroy(qk_plan *p);
+
 /* Run a parsed circuit the way Simulator::run does (src/simulator.cpp:671-706):
  * groups if cfg->is_subcircuit, else gates; *seconds receives the device time
  * of the runner span alone. */

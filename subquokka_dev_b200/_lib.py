@@ -56,6 +56,10 @@ class QkConfig(ctypes.Structure):
     ]
 
 
+class QkPlanOpts(ctypes.Structure):
+    _fields_ = [("dtype", c_int32), ("tile_bits", c_int32), ("reg_bits", c_int32), ("reserved", c_int32 * 5)]
+
+
 class QkError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -90,6 +94,12 @@ PROTOTYPES = {
     "qk_apply_groups": (c_int, [c_void_p, POINTER(QkGate), POINTER(c_int32), c_size_t]),
     "qk_apply_gates_dev": (c_int, [c_void_p, c_int, c_int, POINTER(QkGate), c_size_t, c_void_p]),
     "qk_apply_gates_timed": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(ctypes.c_float)]),
+    "qk_plan_create": (c_int, [POINTER(QkGate), c_size_t, c_int, POINTER(QkPlanOpts), POINTER(c_void_p)]),
+    "qk_plan_create_groups": (c_int, [POINTER(QkGate), POINTER(c_int32), c_size_t, c_int, POINTER(QkPlanOpts),
+                                      POINTER(c_void_p)]),
+    "qk_plan_stats": (c_int, [c_void_p, POINTER(c_size_t), POINTER(c_size_t), POINTER(c_size_t)]),
+    "qk_plan_apply": (c_int, [c_void_p, c_void_p]),
+    "qk_plan_destroy": (None, [c_void_p]),
     "qk_run": (c_int, [POINTER(QkConfig), c_void_p, c_void_p, POINTER(c_double)]),
 }
 

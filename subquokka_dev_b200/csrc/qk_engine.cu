@@ -17,18 +17,34 @@
 
 using namespace qk;
 
+namespace qk {
+struct DevPlan;
+void release_scratch_plan(DevPlan &dp);
+int apply_group_plan(qk_sv *sv, const qk_gate *gates, const int32_t *sizes, size_t ngroups);
+int apply_perm_gate(void *state, int n, int dtype, const Op &op, cudaStream_t st);
+}  // namespace qk
+
+// qk_pass.cu's DevPlan, defined there; the state keeps one as scratch for the
+// subcircuit path (device copy of the last group plan's programs).
+#include "qk_devplan.h"
+
 struct qk_sv {
     int n = 0;
     int dtype = QK_C128;
     void *d = nullptr;
     size_t bytes = 0;
     cudaStream_t stream = nullptr;
-    Op *d_ops = nullptr;     // device copy of the tile ops of the last group call
-    size_t ops_cap = 0;
+    qk::DevPlan scratch;
     int device = 0;
 };
 
 namespace qk {
+
+DevPlan &state_scratch_plan(qk_sv *sv) { return sv->scratch; }
+cudaStream_t state_stream(const qk_sv *sv) { return sv->stream; }
+void *state_ptr(const qk_sv *sv) { return sv->d; }
+int state_qubits(const qk_sv *sv) { return sv->n; }
+int state_dtype(const qk_sv *sv) { return sv->dtype; }
 
 __global__ void k_c128_to_c64(const double2 *in, float2 *out, uint64_t namp) {
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < namp; e += (uint64_t)gridDim.x * blockDim.x)
@@ -63,71 +79,6 @@ static int num_sms() {
 
 static unsigned sweep_blocks(uint64_t items) {
     return (unsigned)std::max<uint64_t>(1, (items + kBlock * kUnroll - 1) / (kBlock * kUnroll));
-}
-
-// ---- tile passes ------------------------------------------------------------
-
-template <typename C> constexpr int tile_default_bits() { return sizeof(C) == 16 ? 12 : 13; }  // 64 KiB
-template <typename C> constexpr int tile_max_bits() { return sizeof(C) == 16 ? 13 : 14; }      // 128 KiB
-
-// Choose tile bits: the given qubits, the low bits 0..4 (512-byte runs for
-// complex128), then further low bits until the default tile size is reached.
-// Returns false when the qubits do not fit in one tile.
-template <typename C>
-static bool build_tile(int n, const std::vector<int> &qubits, TileDesc &d, int *local_of) {
-    std::vector<char> in(n, 0);
-    int cnt = 0;
-    for (int q : qubits)
-        if (!in[q]) { in[q] = 1; ++cnt; }
-    for (int q = 0; q < std::min(n, 5); ++q)
-        if (!in[q]) { in[q] = 1; ++cnt; }
-    const int want = std::min(n, tile_default_bits<C>());
-    for (int q = 0; q < n && cnt < want; ++q)
-        if (!in[q]) { in[q] = 1; ++cnt; }
-    if (cnt > tile_max_bits<C>()) return false;
-    std::memset(&d, 0, sizeof d);
-    d.nbits = n;
-    int k = 0;
-    for (int q = 0; q < n; ++q)
-        if (in[q]) { local_of[q] = k; d.bpos[k++] = q; }
-    d.T = k;
-    d.L = 0;
-    while (d.L < k && d.bpos[d.L] == d.L) ++d.L;
-    return true;
-}
-
-template <typename C>
-static int launch_tile(C *s, int n, const TileDesc &d, const Op *d_ops, int nops, cudaStream_t st) {
-    static bool attr_set = false;
-    const size_t smem = sizeof(C) << d.T;
-    if (!attr_set) {
-        QK_CUDA(cudaFuncSetAttribute(k_tile<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(C) << tile_max_bits<C>())));
-        attr_set = true;
-    }
-    const uint64_t ntiles = 1ull << (n - d.T);
-    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)num_sms() * 4);
-    k_tile<C><<<grid, kTileThreads, smem, st>>>(s, ntiles, d, d_ops, nops);
-    QK_CUDA(cudaGetLastError());
-    return QK_OK;
-}
-
-// Flat permutation sweep, used only when a VSWAP's qubits do not fit in a tile.
-template <typename C>
-__global__ void k_perm_flat(C *__restrict__ s, uint64_t namp, int k, TileDesc pairs) {
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < namp; e += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t f = e;
-        for (int i = 0; i < k; ++i) {
-            const uint64_t a = (e >> pairs.perm_a[i]) & 1, b = (e >> pairs.perm_b[i]) & 1;
-            f = (f & ~(1ull << pairs.perm_a[i]) & ~(1ull << pairs.perm_b[i])) | (b << pairs.perm_a[i]) |
-                (a << pairs.perm_b[i]);
-        }
-        if (e < f) {
-            const C a = s[e];
-            s[e] = s[f];
-            s[f] = a;
-        }
-    }
 }
 
 // ---- per-gate dispatch ------------------------------------------------------
@@ -172,31 +123,10 @@ static int launch_op(C *s, int n, const Op &op, cudaStream_t st) {
         k_swap2<C><<<sweep_blocks(namp / 4), kBlock, 0, st>>>(s, namp / 4, a, b);
         break;
     }
-    case OP_PERM: {
-        // A VSWAP is a pure permutation: stage a tile holding the swapped
-        // qubits and write it back permuted, so reads and writes stay coalesced.
-        const int k = op.nq / 2;
-        std::vector<int> qs(op.q, op.q + op.nq);
-        TileDesc d;
-        std::vector<int> local(n, -1);
-        if (build_tile<C>(n, qs, d, local.data())) {
-            d.nperm = k;
-            for (int i = 0; i < k; ++i) {
-                d.perm_a[i] = local[op.q[i]];
-                d.perm_b[i] = local[op.q[k + i]];
-            }
-            return launch_tile<C>(s, n, d, nullptr, 0, st);
-        }
-        TileDesc pairs;
-        std::memset(&pairs, 0, sizeof pairs);
-        for (int i = 0; i < k; ++i) {
-            pairs.perm_a[i] = op.q[i];
-            pairs.perm_b[i] = op.q[k + i];
-        }
-        const unsigned grid = (unsigned)std::min<uint64_t>((namp + 255) / 256, (uint64_t)num_sms() * 16);
-        k_perm_flat<C><<<grid, 256, 0, st>>>(s, namp, k, pairs);
-        break;
-    }
+    case OP_PERM:
+        // a VSWAP is a pure permutation: a tile pass over the swapped qubits
+        // writes each tile back permuted, reads and writes stay coalesced
+        return apply_perm_gate(s, n, sizeof(C) == sizeof(double2) ? QK_C128 : QK_C64, op, st);
     default:
         return fail(QK_ERR_ARG, "unknown op kind %d", op.kind);
     }
@@ -214,77 +144,6 @@ static int apply_gates_t(C *s, int n, const qk_gate *gates, size_t ng, cudaStrea
             if (op.q[k] < 0 || op.q[k] >= n)
                 return fail(QK_ERR_QUBIT, "gate %zu: qubit %d outside a %d-qubit state", i, op.q[k], n);
         rc = launch_op<C>(s, n, op, st);
-        if (rc) return rc;
-    }
-    return QK_OK;
-}
-
-static bool is_vswap(const qk_gate &g) { return g.kind == QK_GATE_VSWAP || g.kind == QK_GATE_MPI_VSWAP; }
-
-template <typename C>
-static int apply_groups_t(qk_sv *sv, const qk_gate *gates, const int32_t *sizes, size_t ngroups) {
-    C *s = static_cast<C *>(sv->d);
-    const int n = sv->n;
-    struct Step {
-        bool tile;
-        size_t first, count;   // gates (per-gate step)
-        TileDesc d;
-        size_t op0;            // first op in the staged list (tile step)
-        int nops;
-    };
-    std::vector<Step> steps;
-    std::vector<Op> staged;
-    size_t g0 = 0;
-    for (size_t gi = 0; gi < ngroups; ++gi) {
-        if (sizes[gi] < 0) return fail(QK_ERR_ARG, "group %zu has negative size", gi);
-        const size_t cnt = (size_t)sizes[gi];
-        if (cnt == 0) continue;
-        std::vector<int> qs;
-        std::vector<Op> ops(cnt);
-        for (size_t j = 0; j < cnt; ++j) {
-            int rc = lower_gate(gates[g0 + j], ops[j]);
-            if (rc) return rc;
-            for (int k = 0; k < ops[j].nq; ++k) {
-                if (ops[j].q[k] < 0 || ops[j].q[k] >= n)
-                    return fail(QK_ERR_QUBIT, "gate %zu: qubit %d outside a %d-qubit state", g0 + j, ops[j].q[k], n);
-                qs.push_back(ops[j].q[k]);
-            }
-        }
-        Step st{};
-        TileDesc d;
-        std::vector<int> local(n, -1);
-        if (!is_vswap(gates[g0]) && build_tile<C>(n, qs, d, local.data())) {
-            st.tile = true;
-            st.d = d;
-            st.op0 = staged.size();
-            st.nops = (int)cnt;
-            for (auto &op : ops) {
-                for (int k = 0; k < op.nq; ++k) op.q[k] = local[op.q[k]];
-                staged.push_back(op);
-            }
-        } else {
-            st.tile = false;
-            st.first = g0;
-            st.count = cnt;
-        }
-        steps.push_back(st);
-        g0 += cnt;
-    }
-    if (!staged.empty()) {
-        if (staged.size() > sv->ops_cap) {
-            if (sv->d_ops) QK_CUDA(cudaFree(sv->d_ops));
-            sv->d_ops = nullptr;
-            sv->ops_cap = 0;
-            size_t cap = std::max<size_t>(staged.size(), 256);
-            QK_CUDA(cudaMalloc(&sv->d_ops, cap * sizeof(Op)));
-            sv->ops_cap = cap;
-        }
-        QK_CUDA(cudaMemcpyAsync(sv->d_ops, staged.data(), staged.size() * sizeof(Op), cudaMemcpyHostToDevice,
-                                sv->stream));
-    }
-    for (const Step &st : steps) {
-        int rc = st.tile ? launch_tile<C>(s, n, st.d, sv->d_ops + st.op0, st.nops, sv->stream)
-                         : apply_gates_t<C>(s, n, gates + st.first, st.count, sv->stream);
         if (rc) return rc;
     }
     return QK_OK;
@@ -324,7 +183,7 @@ int qk_sv_create(int nqubits, int dtype, qk_sv **out) {
 void qk_sv_destroy(qk_sv *sv) {
     if (!sv) return;
     if (sv->d) cudaFree(sv->d);
-    if (sv->d_ops) cudaFree(sv->d_ops);
+    release_scratch_plan(sv->scratch);
     delete sv;
 }
 
@@ -438,8 +297,7 @@ int qk_apply_gates_timed(qk_sv *sv, const qk_gate *gates, size_t n, float *gate_
 
 int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes, size_t ngroups) {
     if (!sv || (!group_sizes && ngroups)) return fail(QK_ERR_ARG, "null argument");
-    if (sv->dtype == QK_C128) return apply_groups_t<double2>(sv, gates, group_sizes, ngroups);
-    return apply_groups_t<float2>(sv, gates, group_sizes, ngroups);
+    return apply_group_plan(sv, gates, group_sizes, ngroups);
 }
 
 int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds) {

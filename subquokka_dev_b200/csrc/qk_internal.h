@@ -51,3 +51,75 @@ struct qk_circuit {
     std::vector<qk_gate> gates;
     std::vector<int32_t> group_sizes;
 };
+
+namespace qk {
+
+// ---------------------------------------------------------------------------
+// Fused passes.  A pass stages tiles of 2^T amplitudes (tile bits bpos[0..T))
+// and runs a small program on them; each thread keeps R = 2^r amplitudes in
+// registers, indexed by r "register" tile bits, the rest of the tile bits
+// index the thread.  Programs are built on the host (qk_plan.cpp).
+// ---------------------------------------------------------------------------
+constexpr int kPassMaxBits = 14;
+constexpr int kPassMaxReg = 5;
+
+enum TOpKind : uint8_t {
+    TOP_REMAP = 0,  // re-distribute the tile: register slot s <- tile bit bits[s]
+    TOP_G1 = 1,     // dense 2x2 on register slot a; coef -> 4 complex
+    TOP_G2 = 2,     // dense 4x4 on register slots a < b (index bit0 = a); coef -> 16 complex
+    TOP_DIAG = 3,   // amplitude *= coef[bit(a) + 2 bit(b)]; a, b are qubit codes
+    TOP_PHASE = 4,  // amplitude *= coef[0] where bit(a) = bit(b) = 1 (Z, P, CP; b may be none)
+};
+
+// Qubit codes of TOP_DIAG / TOP_PHASE: < 0x80 tile-local bit; 0x80 | q global
+// qubit q that is not a tile bit (constant over a tile); 0xFF no qubit (bit =
+// 0 for TOP_DIAG, 1 for TOP_PHASE).
+constexpr uint8_t kOuterFlag = 0x80;
+constexpr uint8_t kNoQubit = 0xFF;
+
+struct TOp {
+    uint8_t kind;
+    uint8_t a, b;
+    uint8_t nbits;
+    uint8_t bits[kPassMaxReg + 3];
+    uint32_t coef;
+};
+static_assert(sizeof(TOp) == 16, "TOp must stay 16 bytes");
+
+struct PassDesc {
+    int32_t T;                    // tile bits
+    int32_t L;                    // tile bits 0..L-1 are state bits 0..L-1 (contiguous runs)
+    int32_t bpos[kPassMaxBits];   // state bit of each tile bit, ascending
+    int32_t prog0, nprog;         // program slice in the plan's op array
+    int32_t coef0, ncoef;         // coefficient slice (complex values) used by the program
+    int32_t perm;                 // 1: a qubit-permutation pass (VSWAP), prog unused
+    int32_t nperm;
+    int32_t perm_a[6], perm_b[6]; // tile-local bit pairs swapped on store (perm passes)
+};
+
+// Host plan: passes + programs + complex coefficient pool (FP64).
+struct HostPlan {
+    int n = 0;
+    int dtype = 0;
+    int T = 0, r = 0;
+    std::vector<PassDesc> passes;
+    std::vector<TOp> ops;
+    std::vector<double> coef;  // (re, im) pairs
+    size_t nremaps = 0, ngates = 0;
+};
+
+struct PlanOptions {
+    int dtype;
+    int tile_bits;   // T
+    int reg_bits;    // r
+};
+
+// Build a fused plan for a flat gate list (greedy tile-bit choice).
+int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, HostPlan &plan);
+// Build one pass per group (the subcircuit path): every group becomes a pass
+// over the union of its qubits; VSWAP groups become permutation passes.
+int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
+                     HostPlan &plan);
+PlanOptions default_plan_options(int dtype, int n);
+
+}  // namespace qk

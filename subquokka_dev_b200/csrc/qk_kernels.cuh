@@ -31,11 +31,11 @@ template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
     return r;
 }
 
-// a*b + c*d
+// a*b + c*d, as four fused multiply-adds per component
 template <typename C> __device__ __forceinline__ C cmul2(C a, C b, C c, C d) {
     C r;
-    r.x = (a.x * b.x - a.y * b.y) + (c.x * d.x - c.y * d.y);
-    r.y = (a.x * b.y + a.y * b.x) + (c.x * d.y + c.y * d.x);
+    r.x = fma(a.x, b.x, fma(-a.y, b.y, fma(c.x, d.x, -c.y * d.y)));
+    r.y = fma(a.x, b.y, fma(a.y, b.x, fma(c.x, d.y, c.y * d.x)));
     return r;
 }
 
@@ -235,168 +235,6 @@ __global__ void __launch_bounds__(kBlock) k_swap2(C *__restrict__ s, uint64_t nq
             s[i | A] = b[u];
             s[i | B] = a[u];
         }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Tile pass: one CTA stages 2^T amplitudes whose index bits are the tile bits
-// bpos[0..T) (bpos[k] = k for k < L, so every run of 2^L amplitudes is
-// contiguous in HBM) into shared memory, applies a list of ops on tile-local
-// qubits, and writes the tile back.  This is the subcircuit path: a whole
-// gate group costs one HBM read and one write (src/MEM_Runner.cpp:172-183
-// does the same per 2^chunk_qbit chunk on the CPU).  A qubit permutation
-// (VSWAP) is applied by writing element j to the position of perm(j).
-// ---------------------------------------------------------------------------
-constexpr int kTileThreads = 512;
-constexpr int kMaxTileBits = 14;
-
-struct TileDesc {
-    int T;                      // tile bits
-    int L;                      // leading contiguous bits 0..L-1
-    int nbits;                  // state qubits
-    int bpos[kMaxTileBits];     // tile bit positions, ascending
-    int nperm;                  // number of (i, j) local bit swaps applied on store
-    int perm_a[6], perm_b[6];   // local bit pairs swapped on store
-};
-
-__device__ __forceinline__ uint64_t tile_base(uint64_t o, const TileDesc &d) {
-    // Spread the outer index o over the non-tile bits: insert a zero at every
-    // tile bit position, lowest first (bit_string, src/MEM_Runner.cpp:90-99).
-    uint64_t x = o << d.L;
-#pragma unroll 1
-    for (int k = d.L; k < d.T; ++k) x = ins0(x, d.bpos[k]);
-    return x;
-}
-
-__device__ __forceinline__ uint64_t tile_off(uint32_t j, const TileDesc &d) {
-    uint64_t g = j & ((1u << d.L) - 1);
-#pragma unroll 1
-    for (int k = d.L; k < d.T; ++k) g |= (uint64_t)((j >> k) & 1) << d.bpos[k];
-    return g;
-}
-
-template <typename C> __device__ void tile_apply(C *tl, int T, const Op &op) {
-    const uint32_t n = 1u << T;
-    switch (op.kind) {
-    case OP_DENSE1: {
-        const int t = op.q[0];
-        const C m0 = mk<C>(op.m[0], op.m[1]), m1 = mk<C>(op.m[2], op.m[3]);
-        const C m2 = mk<C>(op.m[4], op.m[5]), m3 = mk<C>(op.m[6], op.m[7]);
-        for (uint32_t p = threadIdx.x; p < n / 2; p += blockDim.x) {
-            const uint32_t i = (uint32_t)ins0(p, t), k = i | (1u << t);
-            const C a = tl[i], b = tl[k];
-            tl[i] = cmul2(m0, a, m1, b);
-            tl[k] = cmul2(m2, a, m3, b);
-        }
-        break;
-    }
-    case OP_PHASE1: {
-        const int t = op.q[0];
-        const C ph = mk<C>(op.m[0], op.m[1]);
-        for (uint32_t p = threadIdx.x; p < n / 2; p += blockDim.x) {
-            const uint32_t k = (uint32_t)ins0(p, t) | (1u << t);
-            tl[k] = cmul(tl[k], ph);
-        }
-        break;
-    }
-    case OP_DIAG1: {
-        const int t = op.q[0];
-        const C d0 = mk<C>(op.m[0], op.m[1]), d1 = mk<C>(op.m[2], op.m[3]);
-        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) tl[e] = cmul(tl[e], ((e >> t) & 1) ? d1 : d0);
-        break;
-    }
-    case OP_DENSE2: {
-        const int qa = op.q[0], qb = op.q[1];
-        const uint32_t A = 1u << qa, B = 1u << qb;
-        for (uint32_t p = threadIdx.x; p < n / 4; p += blockDim.x) {
-            const uint32_t i = (uint32_t)ins0(ins0(p, qa), qb);
-            const C x0 = tl[i], x1 = tl[i + A], x2 = tl[i + B], x3 = tl[i + A + B];
-            C y[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const double *mr = op.m + 8 * r;
-                y[r] = cadd(cmul2(mk<C>(mr[0], mr[1]), x0, mk<C>(mr[2], mr[3]), x1),
-                            cmul2(mk<C>(mr[4], mr[5]), x2, mk<C>(mr[6], mr[7]), x3));
-            }
-            tl[i] = y[0];
-            tl[i + A] = y[1];
-            tl[i + B] = y[2];
-            tl[i + A + B] = y[3];
-        }
-        break;
-    }
-    case OP_PHASE2: {
-        const int qa = op.q[0], qb = op.q[1];
-        const uint32_t AB = (1u << qa) | (1u << qb);
-        const C ph = mk<C>(op.m[0], op.m[1]);
-        for (uint32_t p = threadIdx.x; p < n / 4; p += blockDim.x) {
-            const uint32_t k = (uint32_t)ins0(ins0(p, qa), qb) | AB;
-            tl[k] = cmul(tl[k], ph);
-        }
-        break;
-    }
-    case OP_DIAG2: {
-        const int qa = op.q[0], qb = op.q[1];
-        C d[4];
-        for (int k = 0; k < 4; ++k) d[k] = mk<C>(op.m[2 * k], op.m[2 * k + 1]);
-        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x)
-            tl[e] = cmul(tl[e], d[((e >> qa) & 1) | (((e >> qb) & 1) << 1)]);
-        break;
-    }
-    case OP_SWAP2: {
-        const int qa = op.q[0] < op.q[1] ? op.q[0] : op.q[1];
-        const int qb = op.q[0] < op.q[1] ? op.q[1] : op.q[0];
-        const uint32_t A = 1u << qa, B = 1u << qb;
-        for (uint32_t p = threadIdx.x; p < n / 4; p += blockDim.x) {
-            const uint32_t i = (uint32_t)ins0(ins0(p, qa), qb);
-            const C a = tl[i | A];
-            tl[i | A] = tl[i | B];
-            tl[i | B] = a;
-        }
-        break;
-    }
-    case OP_PERM: {
-        const int k = op.nq / 2;
-        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
-            uint32_t f = e;
-            for (int i = 0; i < k; ++i) {
-                const uint32_t a = (e >> op.q[i]) & 1, b = (e >> op.q[k + i]) & 1;
-                f = (f & ~(1u << op.q[i]) & ~(1u << op.q[k + i])) | (b << op.q[i]) | (a << op.q[k + i]);
-            }
-            if (e < f) {
-                const C a = tl[e];
-                tl[e] = tl[f];
-                tl[f] = a;
-            }
-        }
-        break;
-    }
-    }
-}
-
-template <typename C>
-__global__ void __launch_bounds__(kTileThreads) k_tile(C *__restrict__ s, uint64_t ntiles, TileDesc d,
-                                                        const Op *__restrict__ ops, int nops) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *tl = reinterpret_cast<C *>(smem_raw);
-    const uint32_t n = 1u << d.T;
-    for (uint64_t o = blockIdx.x; o < ntiles; o += gridDim.x) {
-        const uint64_t base = tile_base(o, d);
-        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) tl[j] = s[base | tile_off(j, d)];
-        __syncthreads();
-        for (int k = 0; k < nops; ++k) {
-            tile_apply(tl, d.T, ops[k]);
-            __syncthreads();
-        }
-        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
-            uint32_t f = j;
-            for (int i = 0; i < d.nperm; ++i) {
-                const uint32_t a = (j >> d.perm_a[i]) & 1, b = (j >> d.perm_b[i]) & 1;
-                f = (f & ~(1u << d.perm_a[i]) & ~(1u << d.perm_b[i])) | (b << d.perm_a[i]) | (a << d.perm_b[i]);
-            }
-            s[base | tile_off(f, d)] = tl[j];
-        }
-        __syncthreads();
     }
 }
 

@@ -1,0 +1,404 @@
+// Host planner for fused passes.
+//
+// The reference gets its speed from cache blocking: subcircuitFinder groups
+// gates whose qubits all sit inside a 2^12-amplitude chunk and inserts VSWAPs
+// to bring other qubits into the chunk (subcircuitFinder/finder.cpp:629-698),
+// and MEM_Runner applies each group chunk by chunk while it is cache-resident
+// (src/MEM_Runner.cpp:172-183).  Here the chunk is a tile of 2^T amplitudes
+// whose index bits can be ANY T qubits (the low ones for coalescing plus the
+// ones the gates need), so no VSWAP is needed: a pass gathers the strided
+// amplitude sets of its tiles straight from HBM.
+//
+// build_plan: greedy passes.  Walk the remaining gates in order; a gate joins
+// the current pass if none of its qubits is blocked (an earlier gate on that
+// qubit was left out) and, unless it is diagonal, its qubits fit in the tile
+// bit set; otherwise its qubits become blocked.  Diagonal gates (Z, P, RZ, CP,
+// RZZ) join any pass: a qubit outside the tile is constant over a tile.
+//
+// compile_pass: each thread holds 2^r amplitudes indexed by r "register" tile
+// bits.  Ready gates (all earlier gates on their qubits done) run while their
+// qubits are register bits; diagonal gates run at any time; when no ready gate
+// can run the tile is re-distributed through shared memory (TOP_REMAP) so that
+// the qubits of the next ready gates become register bits.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "qk_internal.h"
+
+namespace qk {
+
+PlanOptions default_plan_options(int dtype, int n) {
+    PlanOptions o;
+    o.dtype = dtype;
+    o.tile_bits = std::min(n, dtype == QK_C128 ? 12 : 13);
+    o.reg_bits = std::min(o.tile_bits, dtype == QK_C128 ? 3 : 4);
+    return o;
+}
+
+namespace {
+
+int low_bits(int dtype) { return dtype == QK_C128 ? 3 : 4; }  // 128-byte runs
+
+void push_c(HostPlan &p, double re, double im) {
+    p.coef.push_back(re);
+    p.coef.push_back(im);
+}
+
+struct PassBuilder {
+    const std::vector<Op> &ops;
+    int n, T, r, L;
+    HostPlan &plan;
+
+    // Emit a pass over tile bits B running ops[idx] (in order, dependencies
+    // already satisfied with respect to everything outside idx).
+    int compile(const std::vector<int> &idx, std::vector<int> B) {
+        std::sort(B.begin(), B.end());
+        PassDesc d;
+        std::memset(&d, 0, sizeof d);
+        d.T = (int)B.size();
+        for (int k = 0; k < d.T; ++k) d.bpos[k] = B[k];
+        d.L = 0;
+        while (d.L < d.T && d.bpos[d.L] == d.L) ++d.L;
+        std::vector<int> local(n, -1);
+        for (int k = 0; k < d.T; ++k) local[B[k]] = k;
+        d.prog0 = (int)plan.ops.size();
+        d.coef0 = (int)(plan.coef.size() / 2);
+
+        // per-qubit queues of the pass's ops (positions in idx)
+        std::vector<std::vector<int>> queue(n);
+        for (size_t i = 0; i < idx.size(); ++i)
+            for (int k = 0; k < ops[idx[i]].nq; ++k) queue[ops[idx[i]].q[k]].push_back((int)i);
+        std::vector<size_t> head(n, 0);
+        std::vector<char> done(idx.size(), 0);
+        auto ready = [&](size_t i) {
+            const Op &op = ops[idx[i]];
+            for (int k = 0; k < op.nq; ++k)
+                if (queue[op.q[k]][head[op.q[k]]] != (int)i) return false;
+            return true;
+        };
+        std::vector<int> Q;  // register slot -> tile-local bit
+        auto in_regs = [&](int lq) { return std::find(Q.begin(), Q.end(), lq) != Q.end(); };
+        size_t ndone = 0;
+        bool mapped = false;
+        size_t done_at_remap = (size_t)-1;
+        while (ndone < idx.size()) {
+            bool progress = true;
+            while (progress) {
+                progress = false;
+                for (size_t i = 0; i < idx.size(); ++i) {
+                    if (done[i] || !ready(i)) continue;
+                    const Op &op = ops[idx[i]];
+                    if (!mapped) continue;  // the first program op is always a TOP_REMAP
+                    if (!op_is_diagonal(op)) {
+                        bool ok = true;
+                        for (int k = 0; k < op.nq; ++k) ok = ok && in_regs(local[op.q[k]]);
+                        if (!ok) continue;
+                    }
+                    emit(op, local, Q);
+                    done[i] = 1;
+                    ++ndone;
+                    for (int k = 0; k < op.nq; ++k) ++head[op.q[k]];
+                    progress = true;
+                }
+            }
+            if (ndone == idx.size()) break;
+            if (mapped && ndone == done_at_remap)
+                return fail(QK_ERR_ARG, "planner: a gate cannot be made register-resident (reg_bits %d)", r);
+            done_at_remap = ndone;
+            // re-map: qubits of ready non-diagonal gates first, then of the
+            // following non-diagonal gates in program order
+            std::vector<int> nq;
+            auto add = [&](const Op &op) {
+                bool fits = true;
+                int need = 0;
+                for (int k = 0; k < op.nq; ++k)
+                    if (std::find(nq.begin(), nq.end(), local[op.q[k]]) == nq.end()) ++need;
+                fits = (int)nq.size() + need <= r;
+                if (!fits) return;
+                for (int k = 0; k < op.nq; ++k)
+                    if (std::find(nq.begin(), nq.end(), local[op.q[k]]) == nq.end()) nq.push_back(local[op.q[k]]);
+            };
+            for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
+                if (!done[i] && ready(i) && !op_is_diagonal(ops[idx[i]])) add(ops[idx[i]]);
+            for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
+                if (!done[i] && !op_is_diagonal(ops[idx[i]])) add(ops[idx[i]]);
+            for (int b = 0; b < d.T && (int)nq.size() < r; ++b)
+                if (std::find(nq.begin(), nq.end(), b) == nq.end()) nq.push_back(b);
+            if (nq.empty()) return fail(QK_ERR_ARG, "planner: no register qubits for a pass");
+            Q = nq;
+            TOp t;
+            std::memset(&t, 0, sizeof t);
+            t.kind = TOP_REMAP;
+            t.nbits = (uint8_t)r;
+            for (int s = 0; s < r; ++s) t.bits[s] = (uint8_t)Q[s];
+            plan.ops.push_back(t);
+            ++plan.nremaps;
+            mapped = true;
+        }
+        d.nprog = (int)plan.ops.size() - d.prog0;
+        d.ncoef = (int)(plan.coef.size() / 2) - d.coef0;
+        // program coefficient indices relative to the pass's slice
+        for (int i = d.prog0; i < d.prog0 + d.nprog; ++i)
+            if (plan.ops[i].kind != TOP_REMAP) plan.ops[i].coef -= (uint32_t)d.coef0;
+        plan.passes.push_back(d);
+        plan.ngates += idx.size();
+        return QK_OK;
+    }
+
+    uint8_t code(int q, const std::vector<int> &local) {
+        return local[q] >= 0 ? (uint8_t)local[q] : (uint8_t)(kOuterFlag | q);
+    }
+
+    void emit(const Op &op, const std::vector<int> &local, const std::vector<int> &Q) {
+        TOp t;
+        std::memset(&t, 0, sizeof t);
+        t.coef = (uint32_t)(plan.coef.size() / 2);
+        auto slot = [&](int q) { return (int)(std::find(Q.begin(), Q.end(), local[q]) - Q.begin()); };
+        switch (op.kind) {
+        case OP_DENSE1:
+            t.kind = TOP_G1;
+            t.a = (uint8_t)slot(op.q[0]);
+            for (int k = 0; k < 4; ++k) push_c(plan, op.m[2 * k], op.m[2 * k + 1]);
+            break;
+        case OP_DENSE2:
+        case OP_SWAP2: {
+            double m[32];
+            if (op.kind == OP_DENSE2) std::memcpy(m, op.m, sizeof m);
+            else {
+                std::memset(m, 0, sizeof m);
+                const int perm[4] = {0, 2, 1, 3};
+                for (int i = 0; i < 4; ++i) m[2 * (4 * perm[i] + i)] = 1.0;
+            }
+            int sa = slot(op.q[0]), sb = slot(op.q[1]);
+            t.kind = TOP_G2;
+            if (sa < sb) {
+                t.a = (uint8_t)sa;
+                t.b = (uint8_t)sb;
+                for (int k = 0; k < 16; ++k) push_c(plan, m[2 * k], m[2 * k + 1]);
+            } else {
+                // index bit 0 must be the lower slot: swap the two index bits
+                t.a = (uint8_t)sb;
+                t.b = (uint8_t)sa;
+                auto sw = [](int i) { return ((i & 1) << 1) | ((i >> 1) & 1); };
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < 4; ++j) {
+                        const int k = 4 * sw(i) + sw(j);
+                        push_c(plan, m[2 * k], m[2 * k + 1]);
+                    }
+            }
+            break;
+        }
+        case OP_PHASE1:
+            t.kind = TOP_PHASE;
+            t.a = code(op.q[0], local);
+            t.b = kNoQubit;
+            push_c(plan, op.m[0], op.m[1]);
+            break;
+        case OP_DIAG1:
+            t.kind = TOP_DIAG;
+            t.a = code(op.q[0], local);
+            t.b = kNoQubit;
+            push_c(plan, op.m[0], op.m[1]); push_c(plan, op.m[2], op.m[3]); push_c(plan, 1, 0); push_c(plan, 1, 0);
+            break;
+        case OP_PHASE2:
+            t.kind = TOP_PHASE;
+            t.a = code(op.q[0], local);
+            t.b = code(op.q[1], local);
+            push_c(plan, op.m[0], op.m[1]);
+            break;
+        case OP_DIAG2:
+            t.kind = TOP_DIAG;
+            t.a = code(op.q[0], local);
+            t.b = code(op.q[1], local);
+            for (int k = 0; k < 4; ++k) push_c(plan, op.m[2 * k], op.m[2 * k + 1]);
+            break;
+        default:
+            break;  // OP_PERM never reaches a compute pass
+        }
+        plan.ops.push_back(t);
+    }
+
+    // Permutation pass (VSWAP_k_k): tile bits = low bits + the swapped qubits.
+    void perm_pass(const Op &op) {
+        PassDesc d;
+        std::memset(&d, 0, sizeof d);
+        const int k = op.nq / 2;
+        std::vector<char> in(n, 0);
+        for (int i = 0; i < op.nq; ++i) in[op.q[i]] = 1;
+        int cnt = op.nq;
+        for (int q = 0; q < n && q < L; ++q)
+            if (!in[q]) { in[q] = 1; ++cnt; }
+        d.perm = 1;
+        d.nperm = k;
+        if (cnt > (plan.dtype == QK_C128 ? 13 : 14)) {
+            // too many qubits for one tile: flat in-place permutation sweep
+            d.perm = 2;
+            for (int i = 0; i < k; ++i) { d.perm_a[i] = op.q[i]; d.perm_b[i] = op.q[k + i]; }
+            plan.passes.push_back(d);
+            return;
+        }
+        std::vector<int> local(n, -1);
+        int t = 0;
+        for (int q = 0; q < n; ++q)
+            if (in[q]) { local[q] = t; d.bpos[t++] = q; }
+        d.T = t;
+        while (d.L < d.T && d.bpos[d.L] == d.L) ++d.L;
+        for (int i = 0; i < k; ++i) { d.perm_a[i] = local[op.q[i]]; d.perm_b[i] = local[op.q[k + i]]; }
+        plan.passes.push_back(d);
+        plan.ngates += 1;
+    }
+
+    // Fill B up to T bits: the low bits first, then the lowest unused qubits.
+    void fill(std::vector<int> &B) {
+        for (int q = 0; q < n && (int)B.size() < T; ++q)
+            if (std::find(B.begin(), B.end(), q) == B.end()) B.push_back(q);
+    }
+
+    // Greedy passes over ops[first..last).
+    int greedy(size_t first, size_t last) {
+        std::vector<size_t> pending;
+        for (size_t i = first; i < last; ++i) pending.push_back(i);
+        while (!pending.empty()) {
+            if (ops[pending[0]].kind == OP_PERM) {
+                perm_pass(ops[pending[0]]);
+                pending.erase(pending.begin());
+                continue;
+            }
+            std::vector<int> B;
+            for (int q = 0; q < std::min(n, L); ++q) B.push_back(q);
+            std::vector<char> blocked(n, 0);
+            std::vector<int> take;
+            std::vector<size_t> rest;
+            for (size_t i : pending) {
+                const Op &op = ops[i];
+                bool blk = false;
+                for (int k = 0; k < op.nq; ++k) blk = blk || blocked[op.q[k]];
+                bool ok = !blk && op.kind != OP_PERM;
+                if (ok && !op_is_diagonal(op)) {
+                    int need = 0;
+                    for (int k = 0; k < op.nq; ++k)
+                        if (std::find(B.begin(), B.end(), op.q[k]) == B.end()) ++need;
+                    ok = (int)B.size() + need <= T;
+                    if (ok)
+                        for (int k = 0; k < op.nq; ++k)
+                            if (std::find(B.begin(), B.end(), op.q[k]) == B.end()) B.push_back(op.q[k]);
+                }
+                if (ok) take.push_back((int)i);
+                else {
+                    for (int k = 0; k < op.nq; ++k) blocked[op.q[k]] = 1;
+                    rest.push_back(i);
+                }
+            }
+            fill(B);
+            int rc = compile(take, B);
+            if (rc) return rc;
+            pending.swap(rest);
+        }
+        return QK_OK;
+    }
+};
+
+int lower_all(const qk_gate *gates, size_t ng, int n, std::vector<Op> &ops) {
+    ops.resize(ng);
+    for (size_t i = 0; i < ng; ++i) {
+        int rc = lower_gate(gates[i], ops[i]);
+        if (rc) return rc;
+        for (int k = 0; k < ops[i].nq; ++k)
+            if (ops[i].q[k] < 0 || ops[i].q[k] >= n)
+                return fail(QK_ERR_QUBIT, "gate %zu: qubit %d outside a %d-qubit state", i, ops[i].q[k], n);
+    }
+    return QK_OK;
+}
+
+// Leading state bits always in the tile; two tile bits stay free for the
+// qubits of any single gate, so every pass takes at least one gate.
+int pass_low_bits(const PlanOptions &o, int n) {
+    if (o.tile_bits >= n) return std::min(n, low_bits(o.dtype));
+    return std::max(0, std::min(low_bits(o.dtype), o.tile_bits - 2));
+}
+
+int check_options(const PlanOptions &o, int n) {
+    if (o.dtype != QK_C128 && o.dtype != QK_C64) return fail(QK_ERR_ARG, "unknown dtype %d", o.dtype);
+    if (o.tile_bits < 1 || o.tile_bits > std::min(n, kPassMaxBits))
+        return fail(QK_ERR_ARG, "tile_bits must be in [1, min(n, %d)], got %d", kPassMaxBits, o.tile_bits);
+    const int max_reg = o.dtype == QK_C128 ? 3 : 4;  // more register-resident amplitudes spill
+    // two register bits at least: a two-qubit gate needs both of its qubits
+    const int min_reg = std::min(2, o.tile_bits);
+    if (o.reg_bits < min_reg || o.reg_bits > std::min(o.tile_bits, max_reg))
+        return fail(QK_ERR_ARG, "reg_bits must be in [%d, min(tile_bits, %d)], got %d", min_reg, max_reg, o.reg_bits);
+    if (o.tile_bits - o.reg_bits > 9)
+        return fail(QK_ERR_ARG, "tile_bits - reg_bits must be <= 9 (512 threads), got %d", o.tile_bits - o.reg_bits);
+    const size_t bytes = (o.dtype == QK_C128 ? 16 : 8) << o.tile_bits;
+    if (bytes > (200u << 10)) return fail(QK_ERR_ARG, "tile of %zu bytes exceeds shared memory", bytes);
+    return QK_OK;
+}
+
+}  // namespace
+
+int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, HostPlan &plan) {
+    int rc = check_options(o, n);
+    if (rc) return rc;
+    std::vector<Op> ops;
+    rc = lower_all(gates, ng, n, ops);
+    if (rc) return rc;
+    plan = HostPlan();
+    plan.n = n;
+    plan.dtype = o.dtype;
+    plan.T = o.tile_bits;
+    plan.r = o.reg_bits;
+    PassBuilder b{ops, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), plan};
+    return b.greedy(0, ops.size());
+}
+
+int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
+                     HostPlan &plan) {
+    int rc = check_options(o, n);
+    if (rc) return rc;
+    size_t ng = 0;
+    for (size_t g = 0; g < ngroups; ++g) {
+        if (sizes[g] < 0) return fail(QK_ERR_ARG, "group %zu has negative size", g);
+        ng += (size_t)sizes[g];
+    }
+    std::vector<Op> ops;
+    rc = lower_all(gates, ng, n, ops);
+    if (rc) return rc;
+    plan = HostPlan();
+    plan.n = n;
+    plan.dtype = o.dtype;
+    plan.T = o.tile_bits;
+    plan.r = o.reg_bits;
+    const int L = pass_low_bits(o, n);
+    PassBuilder b{ops, n, o.tile_bits, o.reg_bits, L, plan};
+    size_t g0 = 0;
+    for (size_t g = 0; g < ngroups; ++g) {
+        const size_t cnt = (size_t)sizes[g];
+        if (!cnt) continue;
+        // one pass per group when the union of its non-diagonal qubits fits a
+        // tile (the reference's requirement that a group sit in one chunk);
+        // otherwise the group is split greedily
+        std::vector<int> B;
+        for (int q = 0; q < std::min(n, L); ++q) B.push_back(q);
+        bool fits = true;
+        for (size_t i = g0; i < g0 + cnt && fits; ++i) {
+            if (ops[i].kind == OP_PERM) { fits = false; break; }
+            if (op_is_diagonal(ops[i])) continue;
+            for (int k = 0; k < ops[i].nq; ++k)
+                if (std::find(B.begin(), B.end(), ops[i].q[k]) == B.end()) B.push_back(ops[i].q[k]);
+            fits = (int)B.size() <= o.tile_bits;
+        }
+        if (fits) {
+            b.fill(B);
+            std::vector<int> idx;
+            for (size_t i = g0; i < g0 + cnt; ++i) idx.push_back((int)i);
+            rc = b.compile(idx, B);
+        } else {
+            rc = b.greedy(g0, g0 + cnt);
+        }
+        if (rc) return rc;
+        g0 += cnt;
+    }
+    return QK_OK;
+}
+
+}  // namespace qk

@@ -194,6 +194,19 @@ class StateVector:
     def reset(self) -> None:
         check(self._lib.qk_sv_reset(self.h))
 
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.namp,), "typestr": "<c16" if self.dtype == QK_C128 else "<c8",
+                "data": (self.device_ptr, False), "version": 3}
+
+    def as_torch(self):
+        """Zero-copy torch view of the device state (complex128/complex64)."""
+        import torch
+        return torch.as_tensor(self, device="cuda")
+
+    def apply_plan(self, plan: "Plan") -> None:
+        plan.apply(self)
+
     def upload(self, state: np.ndarray) -> None:
         a = np.ascontiguousarray(state, dtype=np.complex128)
         if a.size != self.namp:
@@ -219,6 +232,47 @@ class StateVector:
     def apply_groups(self, circuit: Circuit) -> None:
         """Subcircuit path (MEM_Runner::run(vector<vector<Gate*>>&))."""
         check(self._lib.qk_apply_groups(self.h, circuit.gates, circuit.group_sizes, circuit.ngroups))
+
+
+class Plan:
+    """A fused plan: the circuit cut into passes, each one HBM read + write of
+    the state (qk_plan_create / qk_plan_create_groups)."""
+
+    def __init__(self, circuit: Circuit, nqubits: int, dtype="c128", tile_bits: int = 0, reg_bits: int = 0,
+                 groups: bool = False):
+        self._lib = _lib.load()
+        o = _lib.QkPlanOpts()
+        o.dtype = DTYPES[dtype]
+        o.tile_bits = int(tile_bits)
+        o.reg_bits = int(reg_bits)
+        self.h = c_void_p()
+        if groups:
+            check(self._lib.qk_plan_create_groups(circuit.gates, circuit.group_sizes, circuit.ngroups, int(nqubits),
+                                                  byref(o), byref(self.h)))
+        else:
+            check(self._lib.qk_plan_create(circuit.gates, circuit.ngates, int(nqubits), byref(o), byref(self.h)))
+        self.nqubits = int(nqubits)
+        self.dtype = DTYPES[dtype]
+
+    def stats(self):
+        """(passes, program ops, register re-mappings)."""
+        a, b, c = c_size_t(), c_size_t(), c_size_t()
+        check(self._lib.qk_plan_stats(self.h, byref(a), byref(b), byref(c)))
+        return a.value, b.value, c.value
+
+    def apply(self, sv: "StateVector") -> None:
+        check(self._lib.qk_plan_apply(sv.h, self.h))
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.qk_plan_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def apply_gates_dev(ptr: int, nqubits: int, dtype, circuit: Circuit, stream_ptr: int | None = None) -> None:

@@ -1,0 +1,120 @@
+"""Parity of the fused-pass path (qk_plan_*) with the oracle and with the
+per-gate path.  complex128 <= 1e-12; complex64 within FP32 rounding."""
+import numpy as np
+import pytest
+
+import oracle
+from subquokka_dev_b200 import Circuit, Plan, StateVector, circuits, make_gate
+
+pytestmark = pytest.mark.gpu
+
+KINDS1 = ["H", "X", "Y", "Z", "P", "RX", "RY", "RZ", "U1"]
+KINDS2 = ["U2", "SWAP", "CP", "RZZ"]
+
+
+def zero(n):
+    s = np.zeros(1 << n, np.complex128)
+    s[0] = 1
+    return s
+
+
+def run_plan(n, circ, init, dtype="c128", tile=0, reg=0, groups=False):
+    plan = Plan(circ, n, dtype, tile, reg, groups)
+    with StateVector(n, dtype) as sv:
+        if init is not None:
+            sv.upload(init)
+        plan.apply(sv)
+        out = sv.download()
+    plan.close()
+    return out
+
+
+def random_circuit(n, ngates, seed, vswap=True):
+    rng = np.random.default_rng(seed)
+    gates = []
+    for _ in range(ngates):
+        r = rng.random()
+        if vswap and r < 0.03:
+            qs = [int(x) for x in rng.choice(n, 4, replace=False)]
+            gates.append(make_gate("VSWAP", qs))
+        elif r < 0.55:
+            k = KINDS1[rng.integers(len(KINDS1))]
+            q = [int(rng.integers(n))]
+            if k == "U1":
+                z = rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))
+                gates.append(make_gate(k, q, coeff=np.linalg.qr(z)[0]))
+            else:
+                gates.append(make_gate(k, q, rng.uniform(-4, 4)))
+        else:
+            k = KINDS2[rng.integers(len(KINDS2))]
+            q = sorted(int(x) for x in rng.choice(n, 2, replace=False))
+            if k == "U2":
+                z = rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))
+                gates.append(make_gate(k, q, coeff=np.linalg.qr(z)[0]))
+            else:
+                gates.append(make_gate(k, q, rng.uniform(-4, 4)))
+    return Circuit(gates)
+
+
+@pytest.mark.parametrize("tile,reg", [(0, 0), (6, 2), (7, 2), (8, 3), (10, 3), (12, 3), (11, 2), (4, 2)])
+def test_random_gate_mix_c128(tile, reg):
+    n = 15
+    circ = random_circuit(n, 300, 11 + tile + reg)
+    init = circuits.random_state(n, 3)
+    ref = oracle.apply_circuit(init, n, circ)
+    assert np.abs(run_plan(n, circ, init, "c128", tile, reg) - ref).max() <= 1e-12
+
+
+@pytest.mark.parametrize("tile,reg", [(0, 0), (13, 4), (9, 4), (6, 2), (12, 3)])
+def test_random_gate_mix_c64(tile, reg):
+    n = 15
+    circ = random_circuit(n, 300, 21 + tile + reg)
+    init = circuits.random_state(n, 4)
+    ref = oracle.apply_circuit(init, n, circ)
+    assert np.abs(run_plan(n, circ, init, "c64", tile, reg) - ref).max() <= 2e-6
+
+
+@pytest.mark.parametrize("n", [3, 5, 9, 12, 13])
+def test_small_states(n):
+    circ = random_circuit(n, 120, 100 + n, vswap=n >= 4)
+    init = circuits.random_state(n, 5)
+    ref = oracle.apply_circuit(init, n, circ)
+    assert np.abs(run_plan(n, circ, init) - ref).max() <= 1e-12
+    assert np.abs(run_plan(n, circ, init, "c64") - ref).max() <= 2e-6
+
+
+def test_benchmark_circuit_families():
+    n = 18
+    for circ in (circuits.random_u3_cz(n, 10, 7), circuits.qft(n), circuits.hea(n, 4, 8)[0]):
+        ref = oracle.apply_circuit(zero(n), n, circ)
+        assert np.abs(run_plan(n, circ, None) - ref).max() <= 1e-12
+
+
+def test_group_plan_matches_flat():
+    n = 14
+    circ = random_circuit(n, 200, 77)
+    sizes = []
+    left = circ.ngates
+    rng = np.random.default_rng(1)
+    while left:
+        k = int(min(left, rng.integers(1, 20)))
+        sizes.append(k)
+        left -= k
+    grouped = Circuit(circ.gate_list(), sizes)
+    init = circuits.random_state(n, 6)
+    ref = oracle.apply_circuit(init, n, circ)
+    assert np.abs(run_plan(n, grouped, init, groups=True) - ref).max() <= 1e-12
+
+
+def test_plan_reuse_and_large_state():
+    # one plan applied twice on a 30-qubit state equals the per-gate path
+    n = 28
+    circ = circuits.random_u3_cz(n, 6, 9)
+    plan = Plan(circ, n, "c128")
+    with StateVector(n) as a, StateVector(n) as b:
+        plan.apply(a)
+        plan.apply(a)
+        b.apply(circ)
+        b.apply(circ)
+        x, y = a.download(), b.download()
+    assert np.abs(x - y).max() <= 1e-12

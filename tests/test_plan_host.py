@@ -1,0 +1,49 @@
+"""Host side of the fused planner (no GPU): pass counts and option checks."""
+import pytest
+
+import subquokka_dev_b200 as sq
+from subquokka_dev_b200 import Plan, circuits, make_gate
+from subquokka_dev_b200.engine import Circuit
+
+
+def test_random30_is_far_fewer_passes_than_gates():
+    c = circuits.random_u3_cz(30, 20, 2030)
+    passes, ops, remaps = Plan(c, 30, "c128").stats()
+    assert c.ngates == 890
+    assert passes <= 30 and ops >= c.ngates and remaps < ops
+
+
+def test_diagonal_gates_join_any_pass():
+    # CP gates on qubits outside any tile are diagonal: one pass holds them all
+    n = 20
+    c = Circuit([make_gate("CP", [a, a + 1], 0.1 * a) for a in range(n - 1)] +
+                [make_gate("RZ", [q], 0.3) for q in range(n)] + [make_gate("RZZ", [3, 19], 0.2)])
+    assert Plan(c, n, "c128").stats()[0] == 1
+
+
+def test_vswap_becomes_permutation_pass():
+    c = Circuit([make_gate("H", [0]), make_gate("VSWAP", [0, 1, 14, 15]), make_gate("H", [1])])
+    p, ops, _ = Plan(c, 16, "c128").stats()
+    assert p == 3
+
+
+def test_group_plan_one_pass_per_fitting_group():
+    c = Circuit([make_gate("H", [q]) for q in range(6)] + [make_gate("VSWAP", [0, 1, 8, 9])] +
+                [make_gate("U1", [q], coeff=[[0, 1], [1, 0]]) for q in range(4)], [6, 1, 4])
+    assert Plan(c, 12, "c128", groups=True).stats()[0] == 3
+
+
+@pytest.mark.parametrize("dtype,tile,reg", [("c128", 13, 3), ("c128", 12, 4), ("c64", 12, 5), ("c128", 12, 0)])
+def test_bad_options_rejected(dtype, tile, reg):
+    c = circuits.qft(14)
+    if reg == 0:
+        Plan(c, 14, dtype, tile, reg)  # defaults fill zero fields
+        return
+    with pytest.raises(sq.QkError):
+        Plan(c, 14, dtype, tile, reg)
+
+
+def test_plan_rejects_bad_qubits():
+    c = Circuit([make_gate("H", [20])])
+    with pytest.raises(sq.QkError):
+        Plan(c, 10, "c128")
