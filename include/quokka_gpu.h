@@ -219,6 +219,27 @@ int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t 
 int qk_plan_apply(qk_sv *sv, qk_plan *p);
 void qk_plan_destroy(qk_plan *p);
 
+/* ---- fused passes without device allocation --------------------------- */
+
+/* Bytes of device memory, fixed at load time, that hold the pass programs and
+ * coefficients of one qk_apply_fused_noalloc call. */
+#define QK_NOALLOC_SCRATCH_BYTES (1u << 20)
+
+/* No counterpart in the reference (its runner allocates nothing on a GPU).
+ * The fused-pass path for callers that cannot allocate device memory -- a
+ * process whose HBM is all handed to a memory pool or to its own state
+ * vectors, or a loop that must not stall other streams on a cudaMalloc /
+ * cudaFree.  Same result as qk_plan_create + qk_plan_apply with default
+ * options on caller-owned memory (state: 2^nqubits amplitudes of dtype on the
+ * current device; cuda_stream: a cudaStream_t, NULL = default), but the pass
+ * programs go to a fixed __device__ array of QK_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit; a circuit whose programs do
+ * not fit returns QK_ERR_ARG.  The first call on a device looks up that
+ * array's address (make it before any stream capture on the device).  Every
+ * call shares the array and overwrites it: calls that overlap on the GPU
+ * (unordered streams) race; calls on one stream are safe. */
+int qk_apply_fused_noalloc(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n, void *cuda_stream);
+
 /* Run a parsed circuit the way Simulator::run does (src/simulator.cpp:671-706):
  * groups if cfg->is_subcircuit, else gates; *seconds receives the device time
  * of the runner span alone. */

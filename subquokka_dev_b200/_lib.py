@@ -100,6 +100,7 @@ PROTOTYPES = {
     "qk_plan_stats": (c_int, [c_void_p, POINTER(c_size_t), POINTER(c_size_t), POINTER(c_size_t)]),
     "qk_plan_apply": (c_int, [c_void_p, c_void_p]),
     "qk_plan_destroy": (None, [c_void_p]),
+    "qk_apply_fused_noalloc": (c_int, [c_void_p, c_int, c_int, POINTER(QkGate), c_size_t, c_void_p]),
     "qk_run": (c_int, [POINTER(QkConfig), c_void_p, c_void_p, POINTER(c_double)]),
 }
 

@@ -470,6 +470,18 @@ static int run_plan(void *state, int dtype, const HostPlan &hp, const DevPlan &d
     return QK_OK;
 }
 
+// Run a host plan whose programs and coefficients are already in device
+// memory at ops / coef (coefficients in the state's type).
+int run_plan_at(void *state, int dtype, const HostPlan &hp, const TOp *ops, const void *coef, cudaStream_t st) {
+    for (const PassDesc &d : hp.passes) {
+        int rc = dtype == QK_C128
+                     ? launch_pass<double2>((double2 *)state, hp.n, hp.r, d, ops, (const double2 *)coef, st)
+                     : launch_pass<float2>((float2 *)state, hp.n, hp.r, d, ops, (const float2 *)coef, st);
+        if (rc) return rc;
+    }
+    return QK_OK;
+}
+
 }  // namespace qk
 
 using namespace qk;
