@@ -219,6 +219,38 @@ int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t 
 int qk_plan_apply(qk_sv *sv, qk_plan *p);
 void qk_plan_destroy(qk_plan *p);
 
+/* ---- observables and gradients ----------------------------------------- */
+/* No counterpart in the reference, which computes no observables or
+ * gradients: these serve variational workloads built on the same gates. */
+
+/* One real-weighted Pauli string: coeff * i^popcount(x & z) X^x Z^z, i.e.
+ * qubit q carries X if only bit q of x_mask is set, Z if only bit q of
+ * z_mask is set, Y if both are. */
+typedef struct qk_pauli_term {
+    double coeff;
+    uint64_t x_mask;
+    uint64_t z_mask;
+} qk_pauli_term;
+
+/* <psi| H |psi> for H = sum of the terms (one state sweep per distinct
+ * x_mask; the state is not modified). */
+int qk_expval_pauli(qk_sv *sv, const qk_pauli_term *terms, size_t nterms, double *out);
+
+/* Adjoint gradient of <H> after gates[0..ngates) applied to the state in sv.
+ * Gate i with param_index[i] >= 0 is trainable (RX, RY or RZ; its angle is
+ * the current value); gradients of gates sharing an index add up into
+ * grad[index] (nparams entries).  The forward state is uncomputed gate by gate
+ * (U^dag) instead of stored; `checkpoints` forward states (-1: min(8,
+ * ceil(sqrt(ngates))), 0: none) are kept at evenly spaced gates, and when the
+ * backward sweep reaches one, the uncomputed state is replaced by it; *drift
+ * receives the root sum of squared differences found there.  *expval
+ * receives <H>.  On return sv holds the initial state again (uncomputed, or
+ * restored from the first checkpoint).  Device memory: one extra state plus
+ * the checkpoints, allocated for the call. */
+int qk_adjoint_grad(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_t *param_index, size_t nparams,
+                    const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
+                    double *drift);
+
 /* ---- fused passes without device allocation --------------------------- */
 
 /* Bytes of device memory, fixed at load time, that hold the pass programs and

@@ -100,3 +100,44 @@ def run_reference(n: int, circuit_text: str, is_subcircuit: int, init: np.ndarra
         m = re.search(r"^([0-9.eE+-]+)s$", r.stdout, re.M)
         secs = float(m.group(1)) if m else float("nan")
         return np.fromfile(out, dtype=np.complex128), secs
+
+
+def pauli_expval(state: np.ndarray, n: int, terms) -> float:
+    """<psi|H|psi> for terms (coeff, x_mask, z_mask), H = sum coeff i^popcount(x&z) X^x Z^z; FP64 numpy."""
+    psi = np.asarray(state, dtype=np.complex128)
+    idx = np.arange(1 << n, dtype=np.uint64)
+    total = 0.0
+    for c, x, z in terms:
+        src = idx ^ np.uint64(x)
+        sign = 1.0 - 2.0 * (np.bitwise_count(src & np.uint64(z)) & 1)
+        phase = 1j ** (bin(int(x) & int(z)).count("1") % 4)
+        # (P psi)[j] = phase * sign(src) * psi[src] with src = j ^ x
+        pj = phase * sign * psi[src.astype(np.int64)]
+        total += float(c) * float(np.vdot(psi, pj).real)
+    return total
+
+
+def param_shift_grad(pc, params: np.ndarray, terms) -> np.ndarray:
+    """Parameter-shift gradient of <H> for a torch_shim.ParamCircuit whose
+    trainable gates are RX/RY/RZ (exp(-i theta P / 2)): per occurrence,
+    (E(theta + pi/2) - E(theta - pi/2)) / 2; FP64 on the CPU oracle."""
+    n = pc.n
+    z0 = np.zeros(1 << n, np.complex128)
+    z0[0] = 1
+
+    def energy(vals):
+        circ, _ = pc.bind(vals)
+        return pauli_expval(apply_circuit(z0, n, circ), n, terms)
+
+    grad = np.zeros(pc.nparams)
+    for k, (_, _, _, p, _) in enumerate(pc.ops):
+        if p < 0:
+            continue
+        # shift only this occurrence: bind, then edit the gate's angle
+        for sgn in (+1, -1):
+            circ, _ = pc.bind(params)
+            g = circ.gates[k]
+            g.param = g.param + sgn * np.pi / 2
+            e = pauli_expval(apply_circuit(z0, n, circ), n, terms)
+            grad[p] += sgn * e / 2
+    return grad

@@ -60,6 +60,10 @@ class QkPlanOpts(ctypes.Structure):
     _fields_ = [("dtype", c_int32), ("tile_bits", c_int32), ("reg_bits", c_int32), ("reserved", c_int32 * 5)]
 
 
+class QkPauliTerm(ctypes.Structure):
+    _fields_ = [("coeff", c_double), ("x_mask", ctypes.c_uint64), ("z_mask", ctypes.c_uint64)]
+
+
 class QkError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -101,6 +105,9 @@ PROTOTYPES = {
     "qk_plan_apply": (c_int, [c_void_p, c_void_p]),
     "qk_plan_destroy": (None, [c_void_p]),
     "qk_apply_fused_noalloc": (c_int, [c_void_p, c_int, c_int, POINTER(QkGate), c_size_t, c_void_p]),
+    "qk_expval_pauli": (c_int, [c_void_p, POINTER(QkPauliTerm), c_size_t, POINTER(c_double)]),
+    "qk_adjoint_grad": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_int32), c_size_t, POINTER(QkPauliTerm),
+                                c_size_t, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)]),
     "qk_run": (c_int, [POINTER(QkConfig), c_void_p, c_void_p, POINTER(c_double)]),
 }
 

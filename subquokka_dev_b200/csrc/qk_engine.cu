@@ -134,6 +134,11 @@ static int launch_op(C *s, int n, const Op &op, cudaStream_t st) {
     return QK_OK;
 }
 
+// One lowered op on a raw state (used by the adjoint sweep).
+int launch_gate_op(void *state, int n, int dtype, const Op &op, cudaStream_t st) {
+    return dtype == QK_C128 ? launch_op<double2>((double2 *)state, n, op, st) : launch_op<float2>((float2 *)state, n, op, st);
+}
+
 template <typename C>
 static int apply_gates_t(C *s, int n, const qk_gate *gates, size_t ng, cudaStream_t st) {
     for (size_t i = 0; i < ng; ++i) {

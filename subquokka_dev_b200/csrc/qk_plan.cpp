@@ -45,6 +45,24 @@ void push_c(HostPlan &p, double re, double im) {
     p.coef.push_back(im);
 }
 
+// Shared-memory bytes a pass program may use: the kernel keeps the program
+// and its coefficients next to the (double-buffered) tile.
+size_t program_budget(int dtype, int T) {
+    const size_t tile = (dtype == QK_C128 ? 16 : 8) << T;
+    const size_t tiles = 2 * tile <= (200u << 10) ? 2 * tile : tile;
+    const size_t avail = (220u << 10) - tiles;
+    return std::min<size_t>(64u << 10, avail - (8u << 10));
+}
+
+// Bytes of program and coefficients one op adds (remaps: 25 % headroom).
+size_t op_cost(const Op &op, int dtype) {
+    const size_t c = dtype == QK_C128 ? 16 : 8;
+    size_t ncoef = 4;
+    if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2) ncoef = 16;
+    else if (op.kind == OP_PHASE1 || op.kind == OP_PHASE2) ncoef = 1;
+    return (16 + ncoef * c) * 5 / 4;
+}
+
 struct PassBuilder {
     const std::vector<Op> &ops;
     int n, T, r, L;
@@ -270,11 +288,13 @@ struct PassBuilder {
             std::vector<char> blocked(n, 0);
             std::vector<int> take;
             std::vector<size_t> rest;
+            const size_t budget = program_budget(plan.dtype, T);
+            size_t used = 0;
             for (size_t i : pending) {
                 const Op &op = ops[i];
                 bool blk = false;
                 for (int k = 0; k < op.nq; ++k) blk = blk || blocked[op.q[k]];
-                bool ok = !blk && op.kind != OP_PERM;
+                bool ok = !blk && op.kind != OP_PERM && (take.empty() || used + op_cost(op, plan.dtype) <= budget);
                 if (ok && !op_is_diagonal(op)) {
                     int need = 0;
                     for (int k = 0; k < op.nq; ++k)
@@ -284,8 +304,10 @@ struct PassBuilder {
                         for (int k = 0; k < op.nq; ++k)
                             if (std::find(B.begin(), B.end(), op.q[k]) == B.end()) B.push_back(op.q[k]);
                 }
-                if (ok) take.push_back((int)i);
-                else {
+                if (ok) {
+                    take.push_back((int)i);
+                    used += op_cost(op, plan.dtype);
+                } else {
                     for (int k = 0; k < op.nq; ++k) blocked[op.q[k]] = 1;
                     rest.push_back(i);
                 }
@@ -380,8 +402,11 @@ int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups,
         std::vector<int> B;
         for (int q = 0; q < std::min(n, L); ++q) B.push_back(q);
         bool fits = true;
+        size_t used = 0;
         for (size_t i = g0; i < g0 + cnt && fits; ++i) {
             if (ops[i].kind == OP_PERM) { fits = false; break; }
+            used += op_cost(ops[i], o.dtype);
+            if (used > program_budget(o.dtype, o.tile_bits)) { fits = false; break; }
             if (op_is_diagonal(ops[i])) continue;
             for (int k = 0; k < ops[i].nq; ++k)
                 if (std::find(B.begin(), B.end(), ops[i].q[k]) == B.end()) B.push_back(ops[i].q[k]);

@@ -275,6 +275,50 @@ class Plan:
             pass
 
 
+# ---------------------------------------------------------------------------
+# observables and gradients
+# ---------------------------------------------------------------------------
+def pauli_terms(terms) -> "ctypes.Array":
+    """[(coeff, x_mask, z_mask), ...] -> qk_pauli_term array."""
+    tl = list(terms)
+    arr = (_lib.QkPauliTerm * max(1, len(tl)))()
+    for i, (c, x, z) in enumerate(tl):
+        arr[i].coeff = float(c)
+        arr[i].x_mask = int(x)
+        arr[i].z_mask = int(z)
+    arr._n = len(tl)
+    return arr
+
+
+def zz_x_hamiltonian(n: int, J, h):
+    """H = sum_i J_i Z_i Z_{i+1} + sum_i h_i X_i as (coeff, x_mask, z_mask) terms."""
+    terms = [(float(J[i]), 0, (1 << i) | (1 << (i + 1))) for i in range(n - 1)]
+    terms += [(float(h[i]), 1 << i, 0) for i in range(n)]
+    return terms
+
+
+def expval(sv: "StateVector", terms) -> float:
+    arr = pauli_terms(terms)
+    out = c_double()
+    check(_lib.load().qk_expval_pauli(sv.h, arr, arr._n, byref(out)))
+    return out.value
+
+
+def adjoint_grad(sv: "StateVector", circuit: Circuit, param_index, nparams: int, terms, checkpoints: int = -1):
+    """(<H>, gradient, checkpoint drift) of H after `circuit` applied to sv's
+    state; gate i is trainable when param_index[i] >= 0 (RX/RY/RZ)."""
+    pidx = np.ascontiguousarray(param_index, dtype=np.int32)
+    if pidx.size != circuit.ngates:
+        raise ValueError("param_index needs one entry per gate")
+    arr = pauli_terms(terms)
+    grad = np.zeros(max(1, nparams), dtype=np.float64)
+    ev, drift = c_double(), c_double()
+    check(_lib.load().qk_adjoint_grad(sv.h, circuit.gates, circuit.ngates, pidx.ctypes.data_as(POINTER(c_int32)),
+                                      int(nparams), arr, arr._n, int(checkpoints), byref(ev),
+                                      grad.ctypes.data_as(POINTER(c_double)), byref(drift)))
+    return ev.value, grad[:nparams], drift.value
+
+
 def apply_gates_dev(ptr: int, nqubits: int, dtype, circuit: Circuit, stream_ptr: int | None = None) -> None:
     """Per-gate path on caller-owned device memory (e.g. a torch tensor)."""
     check(_lib.load().qk_apply_gates_dev(c_void_p(ptr), int(nqubits), DTYPES[dtype], circuit.gates,
