@@ -48,6 +48,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fused", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other named workloads (QFT-20, HEA-26, 33q c64)")
     return ap.parse_args()
 
 
@@ -263,6 +264,93 @@ def fused_variants(args, circ, exact, plain_ms, alg):
     return out
 
 
+def extra_workloads(args):
+    """The other named workloads, each timed with CUDA events after warm-up:
+    QFT-20 on a seeded random state; the 26-qubit hardware-efficient ansatz
+    (12 layers, 624 parameters, ZZ + X Hamiltonian): <H> + adjoint gradient;
+    the 33-qubit 24-layer random circuit in complex64 (fused passes), its error
+    measured against complex128 on the same circuit family at 28 qubits."""
+    import numpy as np
+    import torch
+    from subquokka_dev_b200 import Plan, StateVector, adjoint_grad, circuits, zz_x_hamiltonian
+    from subquokka_dev_b200.torch_shim import hea_template
+    out = {}
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # QFT-20 (L2-resident 16 MiB state)
+    n = 20
+    init = circuits.random_state(n, 20)
+    qft = circuits.qft(n)
+    sv = StateVector(n)
+    sv.set_stream(stream)
+    plan = Plan(qft, n)
+
+    sv.upload(init)
+    ms_pg = time_device(lambda: sv.apply(qft), 3, 20)
+    ms_fu = time_device(lambda: plan.apply(sv), 3, 20)
+    out["qft20_c128"] = {"gates": qft.ngates, "per_gate_ms": ms_pg, "fused_ms": ms_fu, "passes": plan.stats()[0],
+                         "gates_per_s_per_gate_path": qft.ngates / (ms_pg / 1e3)}
+    sv.close()
+    plan.close()
+
+    # HEA-26 adjoint gradients
+    n, layers = 26, 12
+    pc = hea_template(n, layers)
+    rng = np.random.default_rng(26)
+    params = rng.uniform(-np.pi, np.pi, pc.nparams)
+    terms = zz_x_hamiltonian(n, rng.standard_normal(n - 1), rng.standard_normal(n))
+    circ, idx = pc.bind(params)
+    res = {"qubits": n, "layers": layers, "params": pc.nparams, "gates": circ.ngates}
+    grads = {}
+    for dtype, fused in (("c128", False), ("c128", True), ("c64", True)):
+        sv = StateVector(n, dtype)
+        sv.set_stream(stream)
+        box = {}
+
+        def run():
+            sv.reset()
+            box["r"] = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
+        ms = time_device(run, 1, 2)
+        ev, g, drift = box["r"]
+        grads[(dtype, fused)] = g
+        key = f"{dtype}_{'fused' if fused else 'per_gate'}"
+        res[key] = {"ms": ms, "grads_per_s": pc.nparams / (ms / 1e3), "expval": ev, "drift": drift}
+        sv.close()
+    ref = grads[("c128", False)]
+    for k, g in grads.items():
+        key = f"{k[0]}_{'fused' if k[1] else 'per_gate'}"
+        res[key]["max_rel_grad_err_vs_c128_per_gate"] = float(np.abs(g - ref).max() / np.abs(ref).max())
+    out["hea26_adjoint"] = res
+
+    # 33-qubit c64 fused; error at 28 qubits against complex128
+    n33, l33 = 33, 24
+    c33 = circuits.random_u3_cz(n33, l33, 33)
+    p33 = Plan(c33, n33, "c64")
+    sv = StateVector(n33, "c64")
+    sv.set_stream(stream)
+
+    def run33():
+        sv.reset()
+        p33.apply(sv)
+    ms33 = time_device(run33, 1, 2)
+    sv.close()
+    res33 = {"qubits": n33, "layers": l33, "gates": c33.ngates, "passes": p33.stats()[0], "ms_per_circuit": ms33,
+             "state_bytes": 8 << n33, "method": "fused passes, FP32 CUDA-core arithmetic"}
+    p33.close()
+    c28 = circuits.random_u3_cz(28, l33, 33)
+    a, b = StateVector(28, "c128"), StateVector(28, "c64")
+    a.apply(c28)
+    p28 = Plan(c28, 28, "c64")
+    p28.apply(b)
+    dmax, infid = compare_states(b, a)
+    res33.update({"check_qubits": 28, "max_abs_damp_vs_c128": dmax, "one_minus_fidelity_vs_c128": infid})
+    a.close()
+    b.close()
+    p28.close()
+    out["random33_c64"] = res33
+    return out
+
+
 def our_arm(args, rank, world):
     import numpy as np
     import torch
@@ -339,6 +427,7 @@ def our_arm(args, rank, world):
                                for k, v in per_kernel.items()}}
     launches = args.steps * (circ.ngates + 1)
     variants = {} if args.no_fused else fused_variants(args, circ, sv, ms_per_step, alg)
+    extra = {} if (args.no_extra or rank != 0) else None
 
     # end to end through the public API: host gate records in, final state out to pinned host memory
     e2e = None
@@ -371,6 +460,8 @@ def our_arm(args, rank, world):
                "host_buffer": "pinned" if pinned else "pageable"}
         del host
     sv.close()
+    if extra is None:
+        extra = extra_workloads(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -385,7 +476,7 @@ def our_arm(args, rank, world):
                 "gates_per_s": world * circ.ngates / (ms_per_step / 1e3),
                 "hbm_frac_of_peak": value / peak,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-                "fused": variants,
+                "fused": variants, "workloads": extra,
                 "gpu_launches": launches}
         print(json.dumps(line))
     return 0

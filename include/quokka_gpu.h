@@ -251,6 +251,15 @@ int qk_adjoint_grad(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_
                     const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
                     double *drift);
 
+/* qk_adjoint_grad with fused passes: the gates are cut into segments at the
+ * checkpoints (-1: about sqrt(ngates)/4, at most 8); every segment runs
+ * forward as fused passes and backward as two-state passes that apply the
+ * inverse gates to psi and lambda and take each gradient inside the pass.
+ * Same arguments and results. */
+int qk_adjoint_grad_fused(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_t *param_index, size_t nparams,
+                          const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
+                          double *drift);
+
 /* ---- fused passes without device allocation --------------------------- */
 
 /* Bytes of device memory, fixed at load time, that hold the pass programs and

@@ -108,6 +108,9 @@ PROTOTYPES = {
     "qk_expval_pauli": (c_int, [c_void_p, POINTER(QkPauliTerm), c_size_t, POINTER(c_double)]),
     "qk_adjoint_grad": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_int32), c_size_t, POINTER(QkPauliTerm),
                                 c_size_t, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)]),
+    "qk_adjoint_grad_fused": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_int32), c_size_t,
+                                      POINTER(QkPauliTerm), c_size_t, c_int, POINTER(c_double), POINTER(c_double),
+                                      POINTER(c_double)]),
     "qk_run": (c_int, [POINTER(QkConfig), c_void_p, c_void_p, POINTER(c_double)]),
 }
 

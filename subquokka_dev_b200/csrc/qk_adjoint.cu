@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include "qk_devplan.h"
 #include "qk_internal.h"
 #include "qk_kernels.cuh"
 
@@ -225,29 +226,6 @@ static int apply_h_t(C *out, const C *psi, int n, const std::vector<PauliGroup> 
     return QK_OK;
 }
 
-// U^dag of a lowered op (same kind).
-static void invert_op(Op &op) {
-    auto conj = [&](int k) { op.m[2 * k + 1] = -op.m[2 * k + 1]; };
-    switch (op.kind) {
-    case OP_DENSE1:
-    case OP_DENSE2: {
-        const int d = op.kind == OP_DENSE1 ? 2 : 4;
-        double m[32];
-        for (int r = 0; r < d; ++r)
-            for (int c = 0; c < d; ++c) {
-                m[2 * (r * d + c)] = op.m[2 * (c * d + r)];
-                m[2 * (r * d + c) + 1] = -op.m[2 * (c * d + r) + 1];
-            }
-        std::memcpy(op.m, m, sizeof(double) * 2 * d * d);
-        break;
-    }
-    case OP_PHASE1: case OP_PHASE2: conj(0); break;
-    case OP_DIAG1: conj(0); conj(1); break;
-    case OP_DIAG2: for (int k = 0; k < 4; ++k) conj(k); break;
-    default: break;  // SWAP2 and PERM are their own inverses
-    }
-}
-
 // generator of a trainable gate: 1 X (RX), 2 Y (RY), 3 Z (RZ), 0 not trainable
 static int generator(const qk_gate &g) {
     return g.kind == QK_GATE_RX ? 1 : g.kind == QK_GATE_RY ? 2 : g.kind == QK_GATE_RZ ? 3 : 0;
@@ -358,6 +336,99 @@ static int adjoint_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, 
     return done(QK_OK);
 }
 
+// fused passes (qk_pass.cu)
+int upload_host_plan(const HostPlan &hp, DevPlan &dp, cudaStream_t st);
+int run_forward_plan(void *state, const HostPlan &hp, const DevPlan &dp, cudaStream_t st);
+int run_adjoint_plan(void *psi, void *lam, int dtype, const HostPlan &hp, const DevPlan &dp, double *ggrad,
+                     cudaStream_t st);
+
+// The same sweep with fused passes: the gates are cut into segments at the
+// checkpoints; each segment runs forward as fused passes and backward as
+// two-state adjoint passes (inverse gates on psi and lambda, gradients taken
+// inside the passes).  At a segment start psi is compared with and restored
+// from the checkpoint.
+template <typename C>
+static int adjoint_fused_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, const int32_t *pidx,
+                           size_t nparams, const std::vector<PauliGroup> &groups, int ncheck, double *expval,
+                           double *grad, double *drift, cudaStream_t st) {
+    const uint64_t namp = 1ull << n;
+    const size_t bytes = sizeof(C) * namp;
+    std::vector<size_t> cut{0};
+    if (ncheck > 0 && ng > 1)
+        for (int k = 1; k <= ncheck; ++k) {
+            size_t c = (size_t)((double)ng * k / (ncheck + 1));
+            if (c > cut.back() && c < ng) cut.push_back(c);
+        }
+    cut.push_back(ng);
+    const size_t nseg = cut.size() - 1;
+    std::vector<HostPlan> fwd(nseg), bwd(nseg);
+    PlanOptions fo = default_plan_options(dtype, n), bo = default_adjoint_options(dtype, n);
+    for (size_t sgi = 0; sgi < nseg; ++sgi) {
+        int rc = build_plan(gates + cut[sgi], cut[sgi + 1] - cut[sgi], n, fo, fwd[sgi]);
+        if (!rc) rc = build_adjoint_plan(gates + cut[sgi], cut[sgi + 1] - cut[sgi], pidx ? pidx + cut[sgi] : nullptr,
+                                         n, bo, bwd[sgi]);
+        if (rc) return rc;
+        for (int32_t p : bwd[sgi].grad_params)
+            if (p < 0 || (size_t)p >= nparams) return fail(QK_ERR_ARG, "parameter %d >= %zu", p, nparams);
+    }
+    std::vector<DevPlan> dfw(nseg), dbw(nseg);
+    C *lam = nullptr, *ck = nullptr;
+    double *dacc = nullptr;
+    auto done = [&](int code) {
+        for (auto &d : dfw) d.release();
+        for (auto &d : dbw) d.release();
+        if (lam) cudaFree(lam);
+        if (ck) cudaFree(ck);
+        if (dacc) cudaFree(dacc);
+        return code;
+    };
+    for (size_t sgi = 0; sgi < nseg; ++sgi) {
+        int rc = upload_host_plan(fwd[sgi], dfw[sgi], st);
+        if (!rc) rc = upload_host_plan(bwd[sgi], dbw[sgi], st);
+        if (rc) return done(rc);
+    }
+    cudaError_t e = cudaMalloc(&lam, bytes);
+    if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(lambda)"));
+    if (nseg > 1) {
+        e = cudaMalloc(&ck, bytes * (nseg - 1));
+        if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(checkpoints)"));
+    }
+    const size_t nacc = nparams + 2;
+    e = cudaMalloc(&dacc, nacc * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
+    if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(accumulators)"));
+    // forward
+    for (size_t sgi = 0; sgi < nseg; ++sgi) {
+        if (sgi > 0) {
+            e = cudaMemcpyAsync(ck + (sgi - 1) * namp, psi, bytes, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return done(cuda_err(e, "checkpoint"));
+        }
+        int rc = run_forward_plan(psi, fwd[sgi], dfw[sgi], st);
+        if (rc) return done(rc);
+    }
+    int rc = apply_h_t<C>(lam, psi, n, groups, st);
+    if (rc) return done(rc);
+    k_dot_re<C><<<red_grid(namp), kRedThreads, 0, st>>>(psi, lam, namp, dacc + nparams);
+    // backward
+    for (size_t sgi = nseg; sgi-- > 0;) {
+        rc = run_adjoint_plan(psi, lam, dtype, bwd[sgi], dbw[sgi], dacc, st);
+        if (rc) return done(rc);
+        if (sgi > 0) {
+            k_dist2<C><<<red_grid(namp), kRedThreads, 0, st>>>(psi, ck + (sgi - 1) * namp, namp, dacc + nparams + 1);
+            e = cudaMemcpyAsync(psi, ck + (sgi - 1) * namp, bytes, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return done(cuda_err(e, "restore checkpoint"));
+        }
+    }
+    std::vector<double> h(nacc);
+    e = cudaMemcpyAsync(h.data(), dacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return done(cuda_err(e, "read results"));
+    if (grad) std::memcpy(grad, h.data(), nparams * sizeof(double));
+    if (expval) *expval = h[nparams];
+    if (drift) *drift = std::sqrt(h[nparams + 1]);
+    return done(QK_OK);
+}
+
 }  // namespace qk
 
 using namespace qk;
@@ -414,6 +485,25 @@ int qk_adjoint_grad(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_
                                   checkpoints, expval, grad, drift, st);
     return adjoint_t<float2>((float2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams, groups,
                              checkpoints, expval, grad, drift, st);
+}
+
+int qk_adjoint_grad_fused(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_t *param_index, size_t nparams,
+                          const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
+                          double *drift) {
+    if (!sv || (!gates && ngates) || (!terms && nterms) || (!grad && nparams))
+        return fail(QK_ERR_ARG, "null argument");
+    const int n = state_qubits(sv);
+    std::vector<PauliGroup> groups;
+    int rc = group_terms(terms, nterms, n, groups);
+    if (rc) return rc;
+    if (checkpoints < 0) checkpoints = std::min<int>(8, (int)std::ceil(std::sqrt((double)ngates)) / 4);
+    const int dtype = state_dtype(sv);
+    cudaStream_t st = state_stream(sv);
+    if (dtype == QK_C128)
+        return adjoint_fused_t<double2>((double2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams,
+                                        groups, checkpoints, expval, grad, drift, st);
+    return adjoint_fused_t<float2>((float2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams, groups,
+                                   checkpoints, expval, grad, drift, st);
 }
 
 }  // extern "C"

@@ -12,13 +12,16 @@ namespace qk {
 struct DevPlan {
     TOp *ops = nullptr;
     void *coef = nullptr;
-    size_t ops_cap = 0, coef_cap = 0;  // bytes
+    int32_t *gparams = nullptr;  // gradient slot -> parameter index (adjoint plans)
+    size_t ops_cap = 0, coef_cap = 0, gparams_cap = 0;  // bytes
     void release() {
         if (ops) cudaFree(ops);
         if (coef) cudaFree(coef);
+        if (gparams) cudaFree(gparams);
         ops = nullptr;
         coef = nullptr;
-        ops_cap = coef_cap = 0;
+        gparams = nullptr;
+        ops_cap = coef_cap = gparams_cap = 0;
     }
 };
 

@@ -22,12 +22,14 @@ enum OpKind : int32_t {
     OP_DIAG2 = 5,   // *= m[b0 + 2 b1]                             (RZZ)
     OP_SWAP2 = 6,   // exchange |01> and |10> of (q[0], q[1])      (SWAP, VSWAP_1_1)
     OP_PERM = 7,    // swap bit q[i] with bit q[k+i], i < k = nq/2 (VSWAP_k_k)
+    OP_GRAD = 8,    // adjoint sweep: grad[aux] += Im <lambda|G|psi>, G on q[0] = X/Y/Z by m[0] = 1/2/3
 };
 
 struct Op {
     int32_t kind;
     int32_t nq;
     int32_t q[QK_MAX_TARGETS];
+    int32_t aux;   // OP_GRAD: parameter index
     double m[32];  // complex coefficients, (re, im) interleaved
 };
 
@@ -69,6 +71,7 @@ enum TOpKind : uint8_t {
     TOP_G2 = 2,     // dense 4x4 on register slots a < b (index bit0 = a); coef -> 16 complex
     TOP_DIAG = 3,   // amplitude *= coef[bit(a) + 2 bit(b)]; a, b are qubit codes
     TOP_PHASE = 4,  // amplitude *= coef[0] where bit(a) = bit(b) = 1 (Z, P, CP; b may be none)
+    TOP_GRAD = 5,   // two-state passes: gacc[coef] += Im <lambda|G|psi>, G = X/Y/Z (b = 1/2/3) on slot a
 };
 
 // Qubit codes of TOP_DIAG / TOP_PHASE: < 0x80 tile-local bit; 0x80 | q global
@@ -92,6 +95,7 @@ struct PassDesc {
     int32_t bpos[kPassMaxBits];   // state bit of each tile bit, ascending
     int32_t prog0, nprog;         // program slice in the plan's op array
     int32_t coef0, ncoef;         // coefficient slice (complex values) used by the program
+    int32_t grad0, ngrad;         // gradient slots of the pass: plan.grad_params[grad0 .. grad0 + ngrad)
     int32_t perm;                 // 1: a qubit-permutation pass (VSWAP), prog unused
     int32_t nperm;
     int32_t perm_a[6], perm_b[6]; // tile-local bit pairs swapped on store (perm passes)
@@ -105,6 +109,8 @@ struct HostPlan {
     std::vector<PassDesc> passes;
     std::vector<TOp> ops;
     std::vector<double> coef;  // (re, im) pairs
+    std::vector<int32_t> grad_params;  // parameter index of each pass's gradient slots
+    int nstates = 1;           // 2: adjoint passes over (psi, lambda)
     size_t nremaps = 0, ngates = 0;
 };
 
@@ -121,5 +127,12 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
                      HostPlan &plan);
 PlanOptions default_plan_options(int dtype, int n);
+// Backward sweep of an adjoint gradient: the inverses of gates[ng-1..0] on
+// (psi, lambda), with the gradient of trainable gates (pidx[i] >= 0) taken
+// just before their inverse.
+int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int n, const PlanOptions &o,
+                       HostPlan &plan);
+PlanOptions default_adjoint_options(int dtype, int n);
+void invert_op(Op &op);
 
 }  // namespace qk

@@ -216,6 +216,29 @@ int lower_gate(const qk_gate &g, Op &op) {
     }
 }
 
+// U^dag of a lowered op (same kind).
+void invert_op(Op &op) {
+    auto conj = [&](int k) { op.m[2 * k + 1] = -op.m[2 * k + 1]; };
+    switch (op.kind) {
+    case OP_DENSE1:
+    case OP_DENSE2: {
+        const int d = op.kind == OP_DENSE1 ? 2 : 4;
+        double m[32];
+        for (int r = 0; r < d; ++r)
+            for (int c = 0; c < d; ++c) {
+                m[2 * (r * d + c)] = op.m[2 * (c * d + r)];
+                m[2 * (r * d + c) + 1] = -op.m[2 * (c * d + r) + 1];
+            }
+        std::memcpy(op.m, m, sizeof(double) * 2 * d * d);
+        break;
+    }
+    case OP_PHASE1: case OP_PHASE2: conj(0); break;
+    case OP_DIAG1: conj(0); conj(1); break;
+    case OP_DIAG2: for (int k = 0; k < 4; ++k) conj(k); break;
+    default: break;  // SWAP2 and PERM are their own inverses
+    }
+}
+
 }  // namespace qk
 
 using namespace qk;

@@ -194,12 +194,46 @@ __device__ __forceinline__ uint32_t bit_set(uint8_t code, uint32_t none, uint64_
     return (tb & m) ? 0xFFFFFFFFu : 0u;
 }
 
-template <typename C, int R>
-__device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc &d, const TOp *prog, const C *coef,
-                                            uint32_t N) {
+// swz index of register element kk under the current mapping
+template <int LOG2R>
+__device__ __forceinline__ uint32_t reg_sidx(int kk, uint32_t stb, const uint32_t (&sb)[LOG2R]) {
+    uint32_t x = stb;
+#pragma unroll
+    for (int q = 0; q < LOG2R; ++q)
+        if ((kk >> q) & 1) x ^= sb[q];
+    return x;
+}
+
+template <typename C> __device__ __forceinline__ double imdot(C l, C a) { return (double)l.x * a.y - (double)l.y * a.x; }
+template <typename C> __device__ __forceinline__ double redot(C l, C a) { return (double)l.x * a.x + (double)l.y * a.y; }
+
+// Im <lambda|G|psi> over this thread's register pairs of slot S (G = X, Y, Z by gen 1, 2, 3).
+template <int S, typename C, int R>
+__device__ __forceinline__ double reg_grad(const C (&v)[R], const C (&w)[R], int gen) {
+    double s = 0;
+    if constexpr ((1 << S) < R) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (k & (1 << S)) continue;
+            const C a0 = v[k], a1 = v[k | (1 << S)], l0 = w[k], l1 = w[k | (1 << S)];
+            if (gen == 1) s += imdot(l0, a1) + imdot(l1, a0);
+            else if (gen == 2) s += redot(l1, a0) - redot(l0, a1);
+            else s += imdot(l0, a0) - imdot(l1, a1);
+        }
+    }
+    return s;
+}
+
+// Run a pass program on one tile (NS = 1) or on the matching tiles of two
+// states (NS = 2: psi in tl/v, lambda in tw/w; every gate acts on both and
+// TOP_GRAD accumulates Im<lambda|G|psi> into gsm).
+template <typename C, int R, int NS>
+__device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const PassDesc &d, const TOp *prog,
+                                            const C *coef, double *gsm, uint32_t N) {
     constexpr int LOG2R = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
     const uint32_t tid = threadIdx.x;
     C v[R];
+    C w[NS == 2 ? R : 1];
     uint32_t bm[kPassMaxReg] = {0, 0, 0, 0, 0};
     uint32_t sb[LOG2R];  // swz of each register slot's tile bit
     uint32_t tb = 0, stb = 0;
@@ -211,11 +245,9 @@ __device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc
             if (mapped) {
 #pragma unroll
                 for (int kk = 0; kk < R; ++kk) {
-                    uint32_t x = stb;
-#pragma unroll
-                    for (int q = 0; q < LOG2R; ++q)
-                        if ((kk >> q) & 1) x ^= sb[q];
+                    const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);
                     tl[x] = v[kk];
+                    if constexpr (NS == 2) tw[x] = w[kk];
                 }
             }
             __syncthreads();
@@ -230,11 +262,9 @@ __device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc
             stb = swz<C>(tb);
 #pragma unroll
             for (int kk = 0; kk < R; ++kk) {
-                uint32_t x = stb;
-#pragma unroll
-                for (int q = 0; q < LOG2R; ++q)
-                    if ((kk >> q) & 1) x ^= sb[q];
+                const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);
                 v[kk] = tl[x];
+                if constexpr (NS == 2) w[kk] = tw[x];
             }
             __syncthreads();
             mapped = true;
@@ -243,27 +273,27 @@ __device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc
         case TOP_G1: {
             const C m0 = coef[op.coef], m1 = coef[op.coef + 1], m2 = coef[op.coef + 2], m3 = coef[op.coef + 3];
             switch (op.a) {
-            case 0: reg_g1<0>(v, m0, m1, m2, m3); break;
-            case 1: reg_g1<1>(v, m0, m1, m2, m3); break;
-            case 2: reg_g1<2>(v, m0, m1, m2, m3); break;
-            case 3: reg_g1<3>(v, m0, m1, m2, m3); break;
-            case 4: reg_g1<4>(v, m0, m1, m2, m3); break;
+#define QK_G1(S)                                                   \
+    case S:                                                        \
+        reg_g1<S>(v, m0, m1, m2, m3);                              \
+        if constexpr (NS == 2) reg_g1<S>(w, m0, m1, m2, m3);       \
+        break;
+            QK_G1(0) QK_G1(1) QK_G1(2) QK_G1(3) QK_G1(4)
+#undef QK_G1
             }
             break;
         }
         case TOP_G2: {
             const C *m = coef + op.coef;
             switch (op.a * 8 + op.b) {
-            case 0 * 8 + 1: reg_g2<0, 1>(v, m); break;
-            case 0 * 8 + 2: reg_g2<0, 2>(v, m); break;
-            case 0 * 8 + 3: reg_g2<0, 3>(v, m); break;
-            case 0 * 8 + 4: reg_g2<0, 4>(v, m); break;
-            case 1 * 8 + 2: reg_g2<1, 2>(v, m); break;
-            case 1 * 8 + 3: reg_g2<1, 3>(v, m); break;
-            case 1 * 8 + 4: reg_g2<1, 4>(v, m); break;
-            case 2 * 8 + 3: reg_g2<2, 3>(v, m); break;
-            case 2 * 8 + 4: reg_g2<2, 4>(v, m); break;
-            case 3 * 8 + 4: reg_g2<3, 4>(v, m); break;
+#define QK_G2(A, B)                                     \
+    case A * 8 + B:                                     \
+        reg_g2<A, B>(v, m);                             \
+        if constexpr (NS == 2) reg_g2<A, B>(w, m);      \
+        break;
+            QK_G2(0, 1) QK_G2(0, 2) QK_G2(0, 3) QK_G2(0, 4) QK_G2(1, 2)
+            QK_G2(1, 3) QK_G2(1, 4) QK_G2(2, 3) QK_G2(2, 4) QK_G2(3, 4)
+#undef QK_G2
             }
             break;
         }
@@ -275,6 +305,7 @@ __device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc
                 const uint32_t idx = ((A >> kk) & 1) | (((B >> kk) & 1) << 1);
                 const C ph = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
                 v[kk] = cmul(v[kk], ph);
+                if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
             }
             break;
         }
@@ -284,7 +315,26 @@ __device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc
             if (!(M & ((R >= 32) ? 0xFFFFFFFFu : ((1u << R) - 1)))) break;
 #pragma unroll
             for (int kk = 0; kk < R; ++kk)
-                if ((M >> kk) & 1) v[kk] = cmul(v[kk], ph);
+                if ((M >> kk) & 1) {
+                    v[kk] = cmul(v[kk], ph);
+                    if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
+                }
+            break;
+        }
+        case TOP_GRAD: {
+            if constexpr (NS == 2) {
+                double g = 0;
+                switch (op.a) {
+                case 0: g = reg_grad<0>(v, w, op.b); break;
+                case 1: g = reg_grad<1>(v, w, op.b); break;
+                case 2: g = reg_grad<2>(v, w, op.b); break;
+                case 3: g = reg_grad<3>(v, w, op.b); break;
+                case 4: g = reg_grad<4>(v, w, op.b); break;
+                }
+#pragma unroll
+                for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+                if ((tid & 31) == 0) atomicAdd(gsm + op.coef, g);
+            }
             break;
         }
         }
@@ -292,32 +342,39 @@ __device__ __forceinline__ void run_program(C *tl, uint64_t base, const PassDesc
     if (mapped) {
 #pragma unroll
         for (int kk = 0; kk < R; ++kk) {
-            uint32_t x = stb;
-#pragma unroll
-            for (int q = 0; q < LOG2R; ++q)
-                if ((kk >> q) & 1) x ^= sb[q];
+            const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);
             tl[x] = v[kk];
+            if constexpr (NS == 2) tw[x] = w[kk];
         }
     }
 }
 
 // nbuf = 2: the next tile is prefetched (cp.async) into the other buffer
 // while the current one is processed; nbuf = 1: load, process, store.
-template <typename C, int R>
-__global__ void __launch_bounds__(kPassThreads) k_pass(C *__restrict__ s, uint64_t ntiles,
+// NS = 2 runs an adjoint pass over psi (s) and lambda (s2) together; the
+// gradient accumulators of the pass live in shared memory and are added to
+// ggrad[gparams[grad0 + i]] once per CTA.
+template <typename C, int R, int NS>
+__global__ void __launch_bounds__(kPassThreads) k_pass(C *__restrict__ s, C *__restrict__ s2, uint64_t ntiles,
                                                        const __grid_constant__ PassDesc d, const TOp *__restrict__ gprog,
-                                                       const C *__restrict__ gcoef, int nbuf) {
+                                                       const C *__restrict__ gcoef, const int32_t *__restrict__ gparams,
+                                                       double *__restrict__ ggrad, int nbuf) {
     constexpr int LOG2R = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *buf0 = reinterpret_cast<C *>(smem_raw);
     const uint32_t N = 1u << d.T;
-    C *buf1 = buf0 + (nbuf > 1 ? N : 0);
+    C *buf0 = reinterpret_cast<C *>(smem_raw);                 // psi, buffer 0
+    C *buf1 = buf0 + (nbuf > 1 ? N : 0);                       // psi, buffer 1
+    C *wuf0 = buf0 + (size_t)N * nbuf;                         // lambda buffers (NS = 2)
+    C *wuf1 = wuf0 + (nbuf > 1 ? N : 0);
     const uint32_t NT = blockDim.x;
-    // the pass program and its coefficients live in shared memory, after the tiles
-    TOp *prog = reinterpret_cast<TOp *>(buf0 + (size_t)N * nbuf);
+    // program, coefficients and gradient accumulators after the tiles
+    TOp *prog = reinterpret_cast<TOp *>(buf0 + (size_t)N * nbuf * NS);
     C *coef = reinterpret_cast<C *>(prog + d.nprog);
+    double *gsm = reinterpret_cast<double *>(coef + d.ncoef);
     for (int i = threadIdx.x; i < d.nprog; i += NT) prog[i] = gprog[d.prog0 + i];
     for (int i = threadIdx.x; i < d.ncoef; i += NT) coef[i] = gcoef[d.coef0 + i];
+    if constexpr (NS == 2)
+        for (int i = threadIdx.x; i < d.ngrad; i += NT) gsm[i] = 0.0;
     if (d.perm) {
         // permutation pass: plain load / permuted store, one buffer
         for (uint64_t o = blockIdx.x; o < ntiles; o += gridDim.x) {
@@ -332,25 +389,55 @@ __global__ void __launch_bounds__(kPassThreads) k_pass(C *__restrict__ s, uint64
     TileAddr<C, LOG2R> ta;
     ta.init(d, NT);
     uint64_t o = blockIdx.x;
-    if (o < ntiles) prefetch_tile<C, R, LOG2R>(buf0, s, pass_base(o, d), ta);
+    if (o < ntiles) {
+        const uint64_t b0 = pass_base(o, d);
+        if constexpr (NS == 2) {
+#pragma unroll
+            for (int u = 0; u < R; ++u) cp_async_amp(wuf0 + ta.sidx(u), s2 + (b0 | ta.g(u)));
+        }
+        prefetch_tile<C, R, LOG2R>(buf0, s, b0, ta);
+    }
     for (int it = 0; o < ntiles; o += gridDim.x, ++it) {
         C *tl = (it & 1) ? buf1 : buf0;
         C *nx = (it & 1) ? buf0 : buf1;
+        C *tw = (it & 1) ? wuf1 : wuf0;
+        C *nw = (it & 1) ? wuf0 : wuf1;
         const uint64_t base = pass_base(o, d);
         cp_async_wait_all();
         __syncthreads();
         const uint64_t on = o + gridDim.x;
-        if (nbuf > 1 && on < ntiles) prefetch_tile<C, R, LOG2R>(nx, s, pass_base(on, d), ta);
-        run_program<C, R>(tl, base, d, prog, coef, N);
+        if (nbuf > 1 && on < ntiles) {
+            const uint64_t bn = pass_base(on, d);
+            if constexpr (NS == 2) {
+#pragma unroll
+                for (int u = 0; u < R; ++u) cp_async_amp(nw + ta.sidx(u), s2 + (bn | ta.g(u)));
+            }
+            prefetch_tile<C, R, LOG2R>(nx, s, bn, ta);
+        }
+        run_program<C, R, NS>(tl, tw, base, d, prog, coef, gsm, N);
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < R; ++u) s[base | ta.g(u)] = tl[ta.sidx(u)];
+        for (int u = 0; u < R; ++u) {
+            s[base | ta.g(u)] = tl[ta.sidx(u)];
+            if constexpr (NS == 2) s2[base | ta.g(u)] = tw[ta.sidx(u)];
+        }
         if (nbuf == 1) {
             __syncthreads();
-            if (on < ntiles) prefetch_tile<C, R, LOG2R>(tl, s, pass_base(on, d), ta);
+            if (on < ntiles) {
+                const uint64_t bn = pass_base(on, d);
+                if constexpr (NS == 2) {
+#pragma unroll
+                    for (int u = 0; u < R; ++u) cp_async_amp(tw + ta.sidx(u), s2 + (bn | ta.g(u)));
+                }
+                prefetch_tile<C, R, LOG2R>(tl, s, bn, ta);
+            }
         }
     }
     cp_async_wait_all();
+    if constexpr (NS == 2) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < d.ngrad; i += NT) atomicAdd(ggrad + gparams[d.grad0 + i], gsm[i]);
+    }
 }
 
 // In-place permutation sweep for a VSWAP whose qubits do not fit in a tile.
@@ -374,51 +461,85 @@ static int cuda_err(cudaError_t e, const char *what) {
     return fail(e == cudaErrorMemoryAllocation ? QK_ERR_OOM : QK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-template <typename C, int R>
-static int launch_pass_r(C *s, int n, const PassDesc &d, const TOp *ops, const C *coef, cudaStream_t st) {
+// Device pointers of one pass launch.
+template <typename C> struct PassArgs {
+    C *s;                    // psi
+    C *s2;                   // lambda (two-state passes), else null
+    const TOp *ops;
+    const C *coef;
+    const int32_t *gparams;  // gradient slot -> parameter (two-state passes)
+    double *ggrad;           // gradient accumulators (two-state passes)
+};
+
+template <typename C, int R, int NS>
+static int launch_pass_r(const PassArgs<C> &a, int n, const PassDesc &d, cudaStream_t st) {
     static int sms = 0;
-    const size_t tile = sizeof(C) << d.T;
-    const int nbuf = 2 * tile <= (200u << 10) ? 2 : 1;
-    const size_t smem = tile * nbuf + d.nprog * sizeof(TOp) + d.ncoef * sizeof(C);
+    const size_t tile = (sizeof(C) << d.T) * NS;
+    const int nbuf = d.perm ? 1 : (2 * tile <= (200u << 10) ? 2 : 1);
+    const size_t smem = tile * nbuf + d.nprog * sizeof(TOp) + d.ncoef * sizeof(C) + (NS == 2 ? d.ngrad * sizeof(double) : 0);
     if (smem > (220u << 10)) return fail(QK_ERR_ARG, "pass needs %zu bytes of shared memory", smem);
     cudaError_t e;
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaFuncSetAttribute(k_pass<C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 << 10);
+        e = cudaFuncSetAttribute(k_pass<C, R, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 << 10);
         if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(k_pass)");
     }
     const uint32_t threads = d.perm ? std::max<uint32_t>(1, std::min<uint32_t>(kPassThreads, 1u << d.T))
                                     : (uint32_t)((1u << d.T) / R);
     if (threads > kPassThreads || threads == 0) return fail(QK_ERR_ARG, "pass of %d tile bits needs %u threads", d.T, threads);
     int mb = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass<C, R>, (int)threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass<C, R, NS>, (int)threads, smem);
     if (e != cudaSuccess || mb < 1) mb = 1;
     const uint64_t ntiles = 1ull << (n - d.T);
     const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sms * mb);
-    k_pass<C, R><<<grid, threads, smem, st>>>(s, ntiles, d, ops, coef, nbuf);
+    k_pass<C, R, NS><<<grid, threads, smem, st>>>(a.s, a.s2, ntiles, d, a.ops, a.coef, a.gparams, a.ggrad, nbuf);
     e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_err(e, "k_pass launch");
 }
 
 template <typename C>
-static int launch_pass(C *s, int n, int r, const PassDesc &d, const TOp *ops, const C *coef, cudaStream_t st) {
-    if (d.perm == 2) {
-        const uint64_t namp = 1ull << n;
-        const unsigned grid = (unsigned)std::min<uint64_t>((namp + 255) / 256, 148ull * 16);
-        k_perm_flat<C><<<grid, 256, 0, st>>>(s, namp, d);
-        cudaError_t e = cudaGetLastError();
-        return e == cudaSuccess ? QK_OK : cuda_err(e, "k_perm_flat launch");
+static int launch_pass(C *s, int n, int r, const PassDesc &d, const TOp *ops, const C *coef, cudaStream_t st,
+                       C *s2 = nullptr, const int32_t *gparams = nullptr, double *ggrad = nullptr) {
+    if (d.perm) {
+        // a permutation pass acts on each state on its own
+        for (C *x : {s, s2}) {
+            if (!x) continue;
+            int rc;
+            if (d.perm == 2) {
+                const uint64_t namp = 1ull << n;
+                const unsigned grid = (unsigned)std::min<uint64_t>((namp + 255) / 256, 148ull * 16);
+                k_perm_flat<C><<<grid, 256, 0, st>>>(x, namp, d);
+                cudaError_t e = cudaGetLastError();
+                rc = e == cudaSuccess ? QK_OK : cuda_err(e, "k_perm_flat launch");
+            } else {
+                PassArgs<C> a{x, nullptr, ops, coef, nullptr, nullptr};
+                rc = launch_pass_r<C, 2, 1>(a, n, d, st);
+            }
+            if (rc) return rc;
+        }
+        return QK_OK;
     }
+    PassArgs<C> a{s, s2, ops, coef, gparams, ggrad};
     // register-resident amplitudes per thread: up to 8 complex128 or 16
-    // complex64 (more would spill)
+    // complex64 per state (more would spill)
+    if (s2) {
+        switch (r) {
+        case 1: return launch_pass_r<C, 2, 2>(a, n, d, st);
+        case 2: return launch_pass_r<C, 4, 2>(a, n, d, st);
+        case 3:
+            if constexpr (sizeof(C) == sizeof(float2)) return launch_pass_r<C, 8, 2>(a, n, d, st);
+            break;
+        }
+        return fail(QK_ERR_ARG, "reg_bits %d unsupported for two-state passes", r);
+    }
     switch (r) {
-    case 1: return launch_pass_r<C, 2>(s, n, d, ops, coef, st);
-    case 2: return launch_pass_r<C, 4>(s, n, d, ops, coef, st);
-    case 3: return launch_pass_r<C, 8>(s, n, d, ops, coef, st);
+    case 1: return launch_pass_r<C, 2, 1>(a, n, d, st);
+    case 2: return launch_pass_r<C, 4, 1>(a, n, d, st);
+    case 3: return launch_pass_r<C, 8, 1>(a, n, d, st);
     case 4:
-        if constexpr (sizeof(C) == sizeof(float2)) return launch_pass_r<C, 16>(s, n, d, ops, coef, st);
+        if constexpr (sizeof(C) == sizeof(float2)) return launch_pass_r<C, 16, 1>(a, n, d, st);
         break;
     }
     return fail(QK_ERR_ARG, "reg_bits %d unsupported", r);
@@ -443,9 +564,22 @@ static int upload_plan(const HostPlan &hp, int dtype, DevPlan &dp, cudaStream_t 
         if (e != cudaSuccess) { dp.coef_cap = 0; return cuda_err(e, "cudaMalloc(plan coefficients)"); }
         dp.coef_cap = cb;
     }
+    const size_t gb = std::max<size_t>(1, hp.grad_params.size()) * sizeof(int32_t);
+    if (gb > dp.gparams_cap) {
+        if (dp.gparams) cudaFree(dp.gparams);
+        dp.gparams = nullptr;
+        e = cudaMalloc(&dp.gparams, gb);
+        if (e != cudaSuccess) { dp.gparams_cap = 0; return cuda_err(e, "cudaMalloc(plan gradient slots)"); }
+        dp.gparams_cap = gb;
+    }
     if (!hp.ops.empty()) {
         e = cudaMemcpyAsync(dp.ops, hp.ops.data(), hp.ops.size() * sizeof(TOp), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return cuda_err(e, "upload plan ops");
+    }
+    if (!hp.grad_params.empty()) {
+        e = cudaMemcpyAsync(dp.gparams, hp.grad_params.data(), hp.grad_params.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_err(e, "upload plan gradient slots");
     }
     if (nc) {
         if (dtype == QK_C128) {
@@ -468,6 +602,25 @@ static int run_plan(void *state, int dtype, const HostPlan &hp, const DevPlan &d
         if (rc) return rc;
     }
     return QK_OK;
+}
+
+// Run a two-state (adjoint) plan over psi and lambda, adding gradients into ggrad.
+int run_adjoint_plan(void *psi, void *lam, int dtype, const HostPlan &hp, const DevPlan &dp, double *ggrad,
+                     cudaStream_t st) {
+    for (const PassDesc &d : hp.passes) {
+        int rc = dtype == QK_C128
+                     ? launch_pass<double2>((double2 *)psi, hp.n, hp.r, d, dp.ops, (const double2 *)dp.coef, st,
+                                            (double2 *)lam, dp.gparams, ggrad)
+                     : launch_pass<float2>((float2 *)psi, hp.n, hp.r, d, dp.ops, (const float2 *)dp.coef, st,
+                                           (float2 *)lam, dp.gparams, ggrad);
+        if (rc) return rc;
+    }
+    return QK_OK;
+}
+
+int upload_host_plan(const HostPlan &hp, DevPlan &dp, cudaStream_t st) { return upload_plan(hp, hp.dtype, dp, st); }
+int run_forward_plan(void *state, const HostPlan &hp, const DevPlan &dp, cudaStream_t st) {
+    return run_plan(state, hp.dtype, hp, dp, st);
 }
 
 // Run a host plan whose programs and coefficients are already in device

@@ -36,6 +36,15 @@ PlanOptions default_plan_options(int dtype, int n) {
     return o;
 }
 
+// Two-state (adjoint) passes hold twice the data per thread and per tile.
+PlanOptions default_adjoint_options(int dtype, int n) {
+    PlanOptions o;
+    o.dtype = dtype;
+    o.tile_bits = std::min(n, dtype == QK_C128 ? 11 : 12);
+    o.reg_bits = std::min(o.tile_bits, dtype == QK_C128 ? 2 : 3);
+    return o;
+}
+
 namespace {
 
 int low_bits(int dtype) { return dtype == QK_C128 ? 3 : 4; }  // 128-byte runs
@@ -47,8 +56,8 @@ void push_c(HostPlan &p, double re, double im) {
 
 // Shared-memory bytes a pass program may use: the kernel keeps the program
 // and its coefficients next to the (double-buffered) tile.
-size_t program_budget(int dtype, int T) {
-    const size_t tile = (dtype == QK_C128 ? 16 : 8) << T;
+size_t program_budget(int dtype, int T, int nstates) {
+    const size_t tile = ((size_t)(dtype == QK_C128 ? 16 : 8) << T) * nstates;
     const size_t tiles = 2 * tile <= (200u << 10) ? 2 * tile : tile;
     const size_t avail = (220u << 10) - tiles;
     return std::min<size_t>(64u << 10, avail - (8u << 10));
@@ -60,6 +69,7 @@ size_t op_cost(const Op &op, int dtype) {
     size_t ncoef = 4;
     if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2) ncoef = 16;
     else if (op.kind == OP_PHASE1 || op.kind == OP_PHASE2) ncoef = 1;
+    else if (op.kind == OP_GRAD) return (16 + 8) * 5 / 4;  // one double accumulator
     return (16 + ncoef * c) * 5 / 4;
 }
 
@@ -67,6 +77,7 @@ struct PassBuilder {
     const std::vector<Op> &ops;
     int n, T, r, L;
     HostPlan &plan;
+    int grad_base = 0;  // first gradient slot of the pass being compiled
 
     // Emit a pass over tile bits B running ops[idx] (in order, dependencies
     // already satisfied with respect to everything outside idx).
@@ -82,6 +93,8 @@ struct PassBuilder {
         for (int k = 0; k < d.T; ++k) local[B[k]] = k;
         d.prog0 = (int)plan.ops.size();
         d.coef0 = (int)(plan.coef.size() / 2);
+        d.grad0 = (int)plan.grad_params.size();
+        grad_base = d.grad0;
 
         // per-qubit queues of the pass's ops (positions in idx)
         std::vector<std::vector<int>> queue(n);
@@ -156,9 +169,10 @@ struct PassBuilder {
         }
         d.nprog = (int)plan.ops.size() - d.prog0;
         d.ncoef = (int)(plan.coef.size() / 2) - d.coef0;
+        d.ngrad = (int)plan.grad_params.size() - d.grad0;
         // program coefficient indices relative to the pass's slice
         for (int i = d.prog0; i < d.prog0 + d.nprog; ++i)
-            if (plan.ops[i].kind != TOP_REMAP) plan.ops[i].coef -= (uint32_t)d.coef0;
+            if (plan.ops[i].kind != TOP_REMAP && plan.ops[i].kind != TOP_GRAD) plan.ops[i].coef -= (uint32_t)d.coef0;
         plan.passes.push_back(d);
         plan.ngates += idx.size();
         return QK_OK;
@@ -179,6 +193,16 @@ struct PassBuilder {
             t.a = (uint8_t)slot(op.q[0]);
             for (int k = 0; k < 4; ++k) push_c(plan, op.m[2 * k], op.m[2 * k + 1]);
             break;
+        case OP_GRAD: {
+            t.kind = TOP_GRAD;
+            t.a = (uint8_t)slot(op.q[0]);
+            t.b = (uint8_t)op.m[0];
+            int k = grad_base;
+            while (k < (int)plan.grad_params.size() && plan.grad_params[k] != op.aux) ++k;
+            if (k == (int)plan.grad_params.size()) plan.grad_params.push_back(op.aux);
+            t.coef = (uint32_t)(k - grad_base);
+            break;
+        }
         case OP_DENSE2:
         case OP_SWAP2: {
             double m[32];
@@ -288,7 +312,7 @@ struct PassBuilder {
             std::vector<char> blocked(n, 0);
             std::vector<int> take;
             std::vector<size_t> rest;
-            const size_t budget = program_budget(plan.dtype, T);
+            const size_t budget = program_budget(plan.dtype, T, plan.nstates);
             size_t used = 0;
             for (size_t i : pending) {
                 const Op &op = ops[i];
@@ -373,6 +397,44 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
     return b.greedy(0, ops.size());
 }
 
+int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int n, const PlanOptions &o,
+                       HostPlan &plan) {
+    int rc = check_options(o, n);
+    if (rc) return rc;
+    const int max_reg = o.dtype == QK_C128 ? 2 : 3;  // two states per thread
+    if (o.reg_bits > max_reg) return fail(QK_ERR_ARG, "adjoint passes take at most %d register bits", max_reg);
+    std::vector<Op> fwd;
+    rc = lower_all(gates, ng, n, fwd);
+    if (rc) return rc;
+    std::vector<Op> ops;
+    ops.reserve(2 * ng);
+    for (size_t i = ng; i-- > 0;) {
+        Op op = fwd[i];
+        if (pidx && pidx[i] >= 0) {
+            const int gen = gates[i].kind == QK_GATE_RX ? 1 : gates[i].kind == QK_GATE_RY ? 2 : gates[i].kind == QK_GATE_RZ ? 3 : 0;
+            if (!gen) return fail(QK_ERR_UNSUPPORTED, "gate %zu: only RX, RY, RZ are trainable", i);
+            Op g;
+            std::memset(&g, 0, sizeof g);
+            g.kind = OP_GRAD;
+            g.nq = 1;
+            g.q[0] = op.q[0];
+            g.m[0] = gen;
+            g.aux = pidx[i];
+            ops.push_back(g);
+        }
+        invert_op(op);
+        ops.push_back(op);
+    }
+    plan = HostPlan();
+    plan.n = n;
+    plan.dtype = o.dtype;
+    plan.T = o.tile_bits;
+    plan.r = o.reg_bits;
+    plan.nstates = 2;
+    PassBuilder b{ops, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), plan};
+    return b.greedy(0, ops.size());
+}
+
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
                      HostPlan &plan) {
     int rc = check_options(o, n);
@@ -406,7 +468,7 @@ int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups,
         for (size_t i = g0; i < g0 + cnt && fits; ++i) {
             if (ops[i].kind == OP_PERM) { fits = false; break; }
             used += op_cost(ops[i], o.dtype);
-            if (used > program_budget(o.dtype, o.tile_bits)) { fits = false; break; }
+            if (used > program_budget(o.dtype, o.tile_bits, 1)) { fits = false; break; }
             if (op_is_diagonal(ops[i])) continue;
             for (int k = 0; k < ops[i].nq; ++k)
                 if (std::find(B.begin(), B.end(), ops[i].q[k]) == B.end()) B.push_back(ops[i].q[k]);

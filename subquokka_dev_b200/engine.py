@@ -304,16 +304,20 @@ def expval(sv: "StateVector", terms) -> float:
     return out.value
 
 
-def adjoint_grad(sv: "StateVector", circuit: Circuit, param_index, nparams: int, terms, checkpoints: int = -1):
+def adjoint_grad(sv: "StateVector", circuit: Circuit, param_index, nparams: int, terms, checkpoints: int = -1,
+                 fused: bool = False):
     """(<H>, gradient, checkpoint drift) of H after `circuit` applied to sv's
-    state; gate i is trainable when param_index[i] >= 0 (RX/RY/RZ)."""
+    state; gate i is trainable when param_index[i] >= 0 (RX/RY/RZ).  fused:
+    fused forward passes and two-state adjoint passes instead of one kernel
+    per gate."""
     pidx = np.ascontiguousarray(param_index, dtype=np.int32)
     if pidx.size != circuit.ngates:
         raise ValueError("param_index needs one entry per gate")
     arr = pauli_terms(terms)
     grad = np.zeros(max(1, nparams), dtype=np.float64)
     ev, drift = c_double(), c_double()
-    check(_lib.load().qk_adjoint_grad(sv.h, circuit.gates, circuit.ngates, pidx.ctypes.data_as(POINTER(c_int32)),
+    fn = _lib.load().qk_adjoint_grad_fused if fused else _lib.load().qk_adjoint_grad
+    check(fn(sv.h, circuit.gates, circuit.ngates, pidx.ctypes.data_as(POINTER(c_int32)),
                                       int(nparams), arr, arr._n, int(checkpoints), byref(ev),
                                       grad.ctypes.data_as(POINTER(c_double)), byref(drift)))
     return ev.value, grad[:nparams], drift.value

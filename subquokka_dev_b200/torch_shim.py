@@ -52,11 +52,11 @@ class ParamCircuit:
 
 class _Expectation(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, params, pc, terms, dtype, checkpoints):
+    def forward(ctx, params, pc, terms, dtype, checkpoints, fused):
         p = params.detach().to("cpu", torch.float64).numpy()
         circ, idx = pc.bind(p)
         with StateVector(pc.n, dtype) as sv:
-            ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, checkpoints)
+            ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, checkpoints, fused)
         ctx.save_for_backward(torch.as_tensor(grad, dtype=params.dtype, device=params.device))
         ctx.drift = drift
         return torch.tensor(ev, dtype=params.dtype, device=params.device)
@@ -64,12 +64,13 @@ class _Expectation(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g):
         (grad,) = ctx.saved_tensors
-        return g * grad, None, None, None, None
+        return g * grad, None, None, None, None, None
 
 
-def expectation(params: torch.Tensor, pc: ParamCircuit, terms, dtype: str = "c128", checkpoints: int = -1):
+def expectation(params: torch.Tensor, pc: ParamCircuit, terms, dtype: str = "c128", checkpoints: int = -1,
+                fused: bool = True):
     """<0| U(params)^dag H U(params) |0> as a differentiable torch scalar."""
-    return _Expectation.apply(params, pc, terms, dtype, checkpoints)
+    return _Expectation.apply(params, pc, terms, dtype, checkpoints, fused)
 
 
 def hea_template(n: int, layers: int) -> ParamCircuit:

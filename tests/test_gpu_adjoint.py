@@ -35,13 +35,14 @@ def hea_problem(n, layers, seed):
     return pc, params, terms
 
 
+@pytest.mark.parametrize("fused", [False, True])
 @pytest.mark.parametrize("checkpoints", [0, 3, -1])
-def test_adjoint_matches_parameter_shift_c128(checkpoints):
+def test_adjoint_matches_parameter_shift_c128(checkpoints, fused):
     n, layers = 9, 3
     pc, params, terms = hea_problem(n, layers, 21)
     circ, idx = pc.bind(params)
     with StateVector(n) as sv:
-        ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, checkpoints)
+        ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, checkpoints, fused)
         back = sv.download()
     ps = oracle.param_shift_grad(pc, params, terms)
     z0 = np.zeros(1 << n, complex)
@@ -52,18 +53,20 @@ def test_adjoint_matches_parameter_shift_c128(checkpoints):
     assert np.abs(back - z0).max() < 1e-12   # the sweep uncomputes back to |0>
 
 
-def test_adjoint_c64_close_to_fp64():
+@pytest.mark.parametrize("fused", [False, True])
+def test_adjoint_c64_close_to_fp64(fused):
     n, layers = 10, 3
     pc, params, terms = hea_problem(n, layers, 22)
     circ, idx = pc.bind(params)
     with StateVector(n, "c64") as sv:
-        ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms)
+        ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
     ps = oracle.param_shift_grad(pc, params, terms)
     assert np.abs(grad - ps).max() <= 1e-4 * np.abs(ps).max()
     assert drift < 1e-4
 
 
-def test_shared_parameters_and_fixed_gates():
+@pytest.mark.parametrize("fused", [False, True])
+def test_shared_parameters_and_fixed_gates(fused):
     # one parameter on several gates, RX included, non-trainable gates of every kind
     n = 7
     pc = ParamCircuit(n)
@@ -81,7 +84,7 @@ def test_shared_parameters_and_fixed_gates():
     terms = random_terms(n, 10, 23)
     circ, idx = pc.bind(params)
     with StateVector(n) as sv:
-        _, grad, _ = adjoint_grad(sv, circ, idx, pc.nparams, terms)
+        _, grad, _ = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
     assert np.abs(grad - oracle.param_shift_grad(pc, params, terms)).max() < 1e-10
 
 
@@ -94,13 +97,14 @@ def test_torch_shim_backward():
     assert np.abs(p.grad.numpy() - oracle.param_shift_grad(pc, params, terms)).max() < 1e-10
 
 
-def test_adjoint_vs_central_differences_larger_state():
+@pytest.mark.parametrize("fused", [False, True])
+def test_adjoint_vs_central_differences_larger_state(fused):
     # 20 qubits: a few parameters checked by central differences on the GPU
     n, layers = 20, 2
     pc, params, terms = hea_problem(n, layers, 25)
     circ, idx = pc.bind(params)
     with StateVector(n) as sv:
-        _, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms)
+        _, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
     eps = 1e-5
     for p in (0, 7, pc.nparams // 2, pc.nparams - 1):
         e = []
@@ -113,3 +117,15 @@ def test_adjoint_vs_central_differences_larger_state():
                 e.append(expval(sv, terms))
         fd = (e[0] - e[1]) / (2 * eps)
         assert abs(fd - grad[p]) <= 1e-6 * max(1.0, abs(grad[p]))
+
+
+def test_fused_and_per_gate_adjoint_agree_at_scale():
+    n, layers = 22, 4
+    pc, params, terms = hea_problem(n, layers, 26)
+    circ, idx = pc.bind(params)
+    out = []
+    for fused in (False, True):
+        with StateVector(n) as sv:
+            out.append(adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused))
+    assert abs(out[0][0] - out[1][0]) < 1e-12
+    assert np.abs(out[0][1] - out[1][1]).max() < 1e-11
