@@ -260,6 +260,41 @@ int qk_adjoint_grad_fused(qk_sv *sv, const qk_gate *gates, size_t ngates, const 
                           const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
                           double *drift);
 
+/* ---- batches of variational circuits ------------------------------------ */
+/* No counterpart in the reference.  Many circuits of different sizes, each
+ * with its own trainable RX/RY/RZ gates and Pauli-sum H: <H> and the adjoint
+ * gradient of every circuit from one CUDA graph.  Step k of the batch is one
+ * persistent kernel launch that runs the k-th fused pass of every circuit. */
+
+typedef struct qk_batch_opts {
+    int32_t dtype;          /* qk_dtype of the states (default complex64)     */
+    int32_t autotune;       /* 1: time candidate tile shapes on the batch and
+                               keep the fastest                                */
+    int32_t tile_bits, reg_bits;          /* forward passes (0 = default)     */
+    int32_t adj_tile_bits, adj_reg_bits;  /* adjoint passes (0 = default)     */
+    int32_t reserved[2];
+} qk_batch_opts;
+
+typedef struct qk_batch qk_batch;
+
+/* Circuit c has nqubits[c] qubits and gate_counts[c] gates (concatenated in
+ * gates); param_index (one entry per gate, concatenated; NULL = none
+ * trainable) indexes that circuit's own param_counts[c] parameters; its H is
+ * term_counts[c] terms (concatenated).  Builds the plans, allocates every
+ * state and captures the graph. */
+int qk_batch_create(int ncirc, const int32_t *nqubits, const qk_gate *gates, const size_t *gate_counts,
+                    const int32_t *param_index, const size_t *param_counts, const qk_pauli_term *terms,
+                    const size_t *term_counts, const qk_batch_opts *opts, qk_batch **out);
+/* Run the graph: every circuit from |0...0>.  expvals[c], grads (all
+ * parameters, circuit by circuit), drift[c] = || uncomputed state - |0..0> ||. */
+int qk_batch_run(qk_batch *b, double *expvals, double *grads, double *drift);
+/* New values of all parameters (circuit by circuit); the next run uses them. */
+int qk_batch_set_params(qk_batch *b, const double *params);
+/* Graph steps, kernel launches per run and the chosen tile shapes. */
+int qk_batch_stats(const qk_batch *b, int *steps, int *launches, int *tile_bits, int *reg_bits, int *adj_tile_bits,
+                   int *adj_reg_bits);
+void qk_batch_destroy(qk_batch *b);
+
 /* ---- fused passes without device allocation --------------------------- */
 
 /* Bytes of device memory, fixed at load time, that hold the pass programs and

@@ -64,6 +64,11 @@ class QkPauliTerm(ctypes.Structure):
     _fields_ = [("coeff", c_double), ("x_mask", ctypes.c_uint64), ("z_mask", ctypes.c_uint64)]
 
 
+class QkBatchOpts(ctypes.Structure):
+    _fields_ = [("dtype", c_int32), ("autotune", c_int32), ("tile_bits", c_int32), ("reg_bits", c_int32),
+                ("adj_tile_bits", c_int32), ("adj_reg_bits", c_int32), ("reserved", c_int32 * 2)]
+
+
 class QkError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -111,6 +116,14 @@ PROTOTYPES = {
     "qk_adjoint_grad_fused": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_int32), c_size_t,
                                       POINTER(QkPauliTerm), c_size_t, c_int, POINTER(c_double), POINTER(c_double),
                                       POINTER(c_double)]),
+    "qk_batch_create": (c_int, [c_int, POINTER(c_int32), POINTER(QkGate), POINTER(c_size_t), POINTER(c_int32),
+                                POINTER(c_size_t), POINTER(QkPauliTerm), POINTER(c_size_t), POINTER(QkBatchOpts),
+                                POINTER(c_void_p)]),
+    "qk_batch_run": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double), POINTER(c_double)]),
+    "qk_batch_set_params": (c_int, [c_void_p, POINTER(c_double)]),
+    "qk_batch_stats": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int),
+                               POINTER(c_int), POINTER(c_int)]),
+    "qk_batch_destroy": (None, [c_void_p]),
     "qk_run": (c_int, [POINTER(QkConfig), c_void_p, c_void_p, POINTER(c_double)]),
 }
 

@@ -101,3 +101,22 @@ def algorithmic_bytes(circuit: Circuit, n: int, amp_bytes: int = 16) -> int:
         else:
             total += 2 * S
     return total
+
+
+def variational_batch(ncirc: int, seed: int, qmin: int = 14, qmax: int = 22, lmin: int = 4, lmax: int = 16):
+    """Batch of hardware-efficient-ansatz circuits of uneven size: qubits
+    uniform in [qmin, qmax], layers uniform in [lmin, lmax], parameters uniform
+    in [-pi, pi), per-circuit H = sum J_i Z_i Z_{i+1} + sum h_i X_i with J, h
+    ~ N(0, 1).  Returns [(ParamCircuit, params, terms), ...]."""
+    from .engine import zz_x_hamiltonian
+    from .torch_shim import hea_template
+    rng = np.random.default_rng(seed)
+    items = []
+    for _ in range(ncirc):
+        n = int(rng.integers(qmin, qmax + 1))
+        layers = int(rng.integers(lmin, lmax + 1))
+        pc = hea_template(n, layers)
+        params = rng.uniform(-math.pi, math.pi, pc.nparams)
+        terms = zz_x_hamiltonian(n, rng.standard_normal(n - 1), rng.standard_normal(n))
+        items.append((pc, params, terms))
+    return items

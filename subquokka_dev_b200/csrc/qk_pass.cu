@@ -19,335 +19,9 @@
 #include "qk_internal.h"
 #include "qk_kernels.cuh"
 #include "qk_devplan.h"
+#include "qk_pass_device.cuh"
 
 namespace qk {
-
-constexpr int kPassThreads = 512;
-
-__device__ __forceinline__ uint64_t pass_base(uint64_t o, const PassDesc &d) {
-    uint64_t x = o << d.L;
-#pragma unroll 1
-    for (int k = d.L; k < d.T; ++k) x = ins0(x, d.bpos[k]);
-    return x;
-}
-
-__device__ __forceinline__ uint64_t pass_off(uint32_t j, const PassDesc &d) {
-    uint64_t g = j & ((1u << d.L) - 1);
-#pragma unroll 1
-    for (int k = d.L; k < d.T; ++k) g |= (uint64_t)((j >> k) & 1) << d.bpos[k];
-    return g;
-}
-
-// Scatter the low bits of v into the set bits of mask, lowest first.
-__device__ __forceinline__ uint32_t deposit_bits(uint32_t v, uint32_t mask) {
-    uint32_t r = 0;
-    while (mask) {
-        const uint32_t low = mask & (0u - mask);
-        if (v & 1) r |= low;
-        v >>= 1;
-        mask ^= low;
-    }
-    return r;
-}
-
-template <int LOG2R>
-__device__ __forceinline__ uint32_t reg_offset(int kk, const uint32_t (&bm)[kPassMaxReg]) {
-    uint32_t x = 0;
-#pragma unroll
-    for (int s = 0; s < LOG2R; ++s)
-        if ((kk >> s) & 1) x |= bm[s];
-    return x;
-}
-
-template <int S, typename C, int R>
-__device__ __forceinline__ void reg_g1(C (&v)[R], const C m0, const C m1, const C m2, const C m3) {
-    if constexpr ((1 << S) < R) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (k & (1 << S)) continue;
-            const C a = v[k], b = v[k | (1 << S)];
-            v[k] = cmul2(m0, a, m1, b);
-            v[k | (1 << S)] = cmul2(m2, a, m3, b);
-        }
-    }
-}
-
-template <int A, int B, typename C, int R>
-__device__ __forceinline__ void reg_g2(C (&v)[R], const C *__restrict__ m) {
-    if constexpr (A < B && (1 << B) < R) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (k & ((1 << A) | (1 << B))) continue;
-            const int k1 = k | (1 << A), k2 = k | (1 << B), k3 = k | (1 << A) | (1 << B);
-            const C x0 = v[k], x1 = v[k1], x2 = v[k2], x3 = v[k3];
-            C y[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-                y[r] = cadd(cmul2(m[4 * r], x0, m[4 * r + 1], x1), cmul2(m[4 * r + 2], x2, m[4 * r + 3], x3));
-            v[k] = y[0];
-            v[k1] = y[1];
-            v[k2] = y[2];
-            v[k3] = y[3];
-        }
-    }
-}
-
-
-// Shared-memory layout of a tile: element j lives at swz(j), which XORs the
-// low index bits with folds of the higher ones.  A warp's lanes differ in
-// three (complex128) or four (complex64) consecutive thread bits wherever the
-// register qubits sit, and the fold sends those bits to distinct banks, so
-// the re-mappings stay (nearly) conflict-free.
-template <typename C> __device__ __forceinline__ uint32_t swz(uint32_t j) {
-    if constexpr (sizeof(C) == 16) {
-        return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9) ^ (j >> 12)) & 7u);
-    } else {
-        return j ^ (((j >> 4) ^ (j >> 8) ^ (j >> 12)) & 15u);
-    }
-}
-
-// Asynchronous global -> shared copy of one amplitude (cp.async, sm_80+).
-template <typename C> __device__ __forceinline__ void cp_async_amp(C *dst_smem, const C *src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
-    if constexpr (sizeof(C) == 16) {
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-    } else {
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-    }
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// Per-thread address tables of a pass.  Thread tid handles tile elements
-// j = tid + u * NT (u < R), i.e. u sits in the top r tile bits.  Both the HBM
-// offset (a bit deposit) and the shared-memory index (swz) are linear over
-// disjoint bit groups, so each is the thread's own part combined with the
-// parts of the set bits of u (compile-time after unrolling).
-template <typename C, int LOG2R> struct TileAddr {
-    uint64_t g_t;                 // HBM offset of tid's bits
-    uint64_t g_u[LOG2R];          // HBM offset of bit b of u
-    uint32_t s_t;                 // swz of tid
-    uint32_t s_u[LOG2R];          // swz of bit b of u
-    __device__ __forceinline__ void init(const PassDesc &d, uint32_t NT) {
-        g_t = pass_off(threadIdx.x, d);
-        s_t = swz<C>(threadIdx.x);
-#pragma unroll
-        for (int b = 0; b < LOG2R; ++b) {
-            g_u[b] = pass_off(NT << b, d);
-            s_u[b] = swz<C>(NT << b);
-        }
-    }
-    __device__ __forceinline__ uint64_t g(int u) const {
-        uint64_t x = g_t;
-#pragma unroll
-        for (int b = 0; b < LOG2R; ++b)
-            if ((u >> b) & 1) x |= g_u[b];
-        return x;
-    }
-    __device__ __forceinline__ uint32_t sidx(int u) const {
-        uint32_t x = s_t;
-#pragma unroll
-        for (int b = 0; b < LOG2R; ++b)
-            if ((u >> b) & 1) x ^= s_u[b];
-        return x;
-    }
-};
-
-template <typename C, int R, int LOG2R>
-__device__ __forceinline__ void prefetch_tile(C *buf, const C *__restrict__ s, uint64_t base,
-                                              const TileAddr<C, LOG2R> &ta) {
-#pragma unroll
-    for (int u = 0; u < R; ++u) cp_async_amp(buf + ta.sidx(u), s + (base | ta.g(u)));
-    cp_async_commit();
-}
-
-// Permutation pass: tile element j goes to the position of perm(j).
-template <typename C>
-__device__ void run_perm_tile(C *__restrict__ s, C *tl, uint64_t base, const PassDesc &d, uint32_t N, uint32_t NT) {
-    for (uint32_t j = threadIdx.x; j < N; j += NT) {
-        uint32_t f = j;
-        for (int i = 0; i < d.nperm; ++i) {
-            const uint32_t a = (j >> d.perm_a[i]) & 1, b = (j >> d.perm_b[i]) & 1;
-            f = (f & ~(1u << d.perm_a[i]) & ~(1u << d.perm_b[i])) | (b << d.perm_a[i]) | (a << d.perm_b[i]);
-        }
-        s[base | pass_off(f, d)] = tl[swz<C>(j)];
-    }
-}
-
-// Bit pattern over the register index kk (R bits) of "register slot s is 1".
-__device__ __forceinline__ uint32_t slot_pattern(int s) {
-    return s == 0 ? 0xAAAAAAAAu : s == 1 ? 0xCCCCCCCCu : s == 2 ? 0xF0F0F0F0u : s == 3 ? 0xFF00FF00u : 0xFFFF0000u;
-}
-
-// For a diagonal-op qubit code: the set of register indices kk at which that
-// qubit's bit is 1, given the current mapping (reg slots -> tile bits, thread
-// bits tb, tile base).
-template <int LOG2R>
-__device__ __forceinline__ uint32_t bit_set(uint8_t code, uint32_t none, uint64_t base, uint32_t tb,
-                                            const uint32_t (&bm)[kPassMaxReg]) {
-    if (code == kNoQubit) return none ? 0xFFFFFFFFu : 0u;
-    if (code & kOuterFlag) return ((base >> (code & 0x7F)) & 1) ? 0xFFFFFFFFu : 0u;
-    const uint32_t m = 1u << code;
-#pragma unroll
-    for (int s = 0; s < LOG2R; ++s)
-        if (bm[s] == m) return slot_pattern(s);
-    return (tb & m) ? 0xFFFFFFFFu : 0u;
-}
-
-// swz index of register element kk under the current mapping
-template <int LOG2R>
-__device__ __forceinline__ uint32_t reg_sidx(int kk, uint32_t stb, const uint32_t (&sb)[LOG2R]) {
-    uint32_t x = stb;
-#pragma unroll
-    for (int q = 0; q < LOG2R; ++q)
-        if ((kk >> q) & 1) x ^= sb[q];
-    return x;
-}
-
-template <typename C> __device__ __forceinline__ double imdot(C l, C a) { return (double)l.x * a.y - (double)l.y * a.x; }
-template <typename C> __device__ __forceinline__ double redot(C l, C a) { return (double)l.x * a.x + (double)l.y * a.y; }
-
-// Im <lambda|G|psi> over this thread's register pairs of slot S (G = X, Y, Z by gen 1, 2, 3).
-template <int S, typename C, int R>
-__device__ __forceinline__ double reg_grad(const C (&v)[R], const C (&w)[R], int gen) {
-    double s = 0;
-    if constexpr ((1 << S) < R) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (k & (1 << S)) continue;
-            const C a0 = v[k], a1 = v[k | (1 << S)], l0 = w[k], l1 = w[k | (1 << S)];
-            if (gen == 1) s += imdot(l0, a1) + imdot(l1, a0);
-            else if (gen == 2) s += redot(l1, a0) - redot(l0, a1);
-            else s += imdot(l0, a0) - imdot(l1, a1);
-        }
-    }
-    return s;
-}
-
-// Run a pass program on one tile (NS = 1) or on the matching tiles of two
-// states (NS = 2: psi in tl/v, lambda in tw/w; every gate acts on both and
-// TOP_GRAD accumulates Im<lambda|G|psi> into gsm).
-template <typename C, int R, int NS>
-__device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const PassDesc &d, const TOp *prog,
-                                            const C *coef, double *gsm, uint32_t N) {
-    constexpr int LOG2R = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
-    const uint32_t tid = threadIdx.x;
-    C v[R];
-    C w[NS == 2 ? R : 1];
-    uint32_t bm[kPassMaxReg] = {0, 0, 0, 0, 0};
-    uint32_t sb[LOG2R];  // swz of each register slot's tile bit
-    uint32_t tb = 0, stb = 0;
-    bool mapped = false;
-    for (int p = 0; p < d.nprog; ++p) {
-        const TOp op = prog[p];
-        switch (op.kind) {
-        case TOP_REMAP: {
-            if (mapped) {
-#pragma unroll
-                for (int kk = 0; kk < R; ++kk) {
-                    const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);
-                    tl[x] = v[kk];
-                    if constexpr (NS == 2) tw[x] = w[kk];
-                }
-            }
-            __syncthreads();
-            uint32_t regmask = 0;
-#pragma unroll
-            for (int q = 0; q < LOG2R; ++q) {
-                bm[q] = 1u << op.bits[q];
-                sb[q] = swz<C>(bm[q]);
-                regmask |= bm[q];
-            }
-            tb = deposit_bits(tid, (N - 1) & ~regmask);
-            stb = swz<C>(tb);
-#pragma unroll
-            for (int kk = 0; kk < R; ++kk) {
-                const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);
-                v[kk] = tl[x];
-                if constexpr (NS == 2) w[kk] = tw[x];
-            }
-            __syncthreads();
-            mapped = true;
-            break;
-        }
-        case TOP_G1: {
-            const C m0 = coef[op.coef], m1 = coef[op.coef + 1], m2 = coef[op.coef + 2], m3 = coef[op.coef + 3];
-            switch (op.a) {
-#define QK_G1(S)                                                   \
-    case S:                                                        \
-        reg_g1<S>(v, m0, m1, m2, m3);                              \
-        if constexpr (NS == 2) reg_g1<S>(w, m0, m1, m2, m3);       \
-        break;
-            QK_G1(0) QK_G1(1) QK_G1(2) QK_G1(3) QK_G1(4)
-#undef QK_G1
-            }
-            break;
-        }
-        case TOP_G2: {
-            const C *m = coef + op.coef;
-            switch (op.a * 8 + op.b) {
-#define QK_G2(A, B)                                     \
-    case A * 8 + B:                                     \
-        reg_g2<A, B>(v, m);                             \
-        if constexpr (NS == 2) reg_g2<A, B>(w, m);      \
-        break;
-            QK_G2(0, 1) QK_G2(0, 2) QK_G2(0, 3) QK_G2(0, 4) QK_G2(1, 2)
-            QK_G2(1, 3) QK_G2(1, 4) QK_G2(2, 3) QK_G2(2, 4) QK_G2(3, 4)
-#undef QK_G2
-            }
-            break;
-        }
-        case TOP_DIAG: {
-            const C d0 = coef[op.coef], d1 = coef[op.coef + 1], d2 = coef[op.coef + 2], d3 = coef[op.coef + 3];
-            const uint32_t A = bit_set<LOG2R>(op.a, 0, base, tb, bm), B = bit_set<LOG2R>(op.b, 0, base, tb, bm);
-#pragma unroll
-            for (int kk = 0; kk < R; ++kk) {
-                const uint32_t idx = ((A >> kk) & 1) | (((B >> kk) & 1) << 1);
-                const C ph = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
-                v[kk] = cmul(v[kk], ph);
-                if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
-            }
-            break;
-        }
-        case TOP_PHASE: {
-            const C ph = coef[op.coef];
-            const uint32_t M = bit_set<LOG2R>(op.a, 1, base, tb, bm) & bit_set<LOG2R>(op.b, 1, base, tb, bm);
-            if (!(M & ((R >= 32) ? 0xFFFFFFFFu : ((1u << R) - 1)))) break;
-#pragma unroll
-            for (int kk = 0; kk < R; ++kk)
-                if ((M >> kk) & 1) {
-                    v[kk] = cmul(v[kk], ph);
-                    if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
-                }
-            break;
-        }
-        case TOP_GRAD: {
-            if constexpr (NS == 2) {
-                double g = 0;
-                switch (op.a) {
-                case 0: g = reg_grad<0>(v, w, op.b); break;
-                case 1: g = reg_grad<1>(v, w, op.b); break;
-                case 2: g = reg_grad<2>(v, w, op.b); break;
-                case 3: g = reg_grad<3>(v, w, op.b); break;
-                case 4: g = reg_grad<4>(v, w, op.b); break;
-                }
-#pragma unroll
-                for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
-                if ((tid & 31) == 0) atomicAdd(gsm + op.coef, g);
-            }
-            break;
-        }
-        }
-    }
-    if (mapped) {
-#pragma unroll
-        for (int kk = 0; kk < R; ++kk) {
-            const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);
-            tl[x] = v[kk];
-            if constexpr (NS == 2) tw[x] = w[kk];
-        }
-    }
-}
 
 // nbuf = 2: the next tile is prefetched (cp.async) into the other buffer
 // while the current one is processed; nbuf = 1: load, process, store.

@@ -323,6 +323,74 @@ def adjoint_grad(sv: "StateVector", circuit: Circuit, param_index, nparams: int,
     return ev.value, grad[:nparams], drift.value
 
 
+class Batch:
+    """Many variational circuits, <H> and adjoint gradients of each, from one
+    CUDA graph (qk_batch_*).  items: [(ParamCircuit, params, terms), ...]."""
+
+    def __init__(self, items, dtype="c64", autotune: bool = False, tile_bits: int = 0, reg_bits: int = 0,
+                 adj_tile_bits: int = 0, adj_reg_bits: int = 0):
+        self._lib = _lib.load()
+        nq, gates, gcount, pidx, pcount, terms, tcount = [], [], [], [], [], [], []
+        self.param_counts = []
+        for pc, params, tl in items:
+            circ, idx = pc.bind(np.asarray(params, dtype=np.float64))
+            nq.append(pc.n)
+            gates += circ.gate_list()
+            gcount.append(circ.ngates)
+            pidx += list(idx)
+            pcount.append(pc.nparams)
+            self.param_counts.append(pc.nparams)
+            terms += list(tl)
+            tcount.append(len(tl))
+        self.ncirc = len(items)
+        self.nparams = int(sum(pcount))
+        self._gates = (QkGate * len(gates))(*gates)
+        arr_t = pauli_terms(terms)
+        o = _lib.QkBatchOpts()
+        o.dtype = DTYPES[dtype]
+        o.autotune = int(autotune)
+        o.tile_bits, o.reg_bits, o.adj_tile_bits, o.adj_reg_bits = tile_bits, reg_bits, adj_tile_bits, adj_reg_bits
+        self.h = c_void_p()
+        check(self._lib.qk_batch_create(
+            self.ncirc, (c_int32 * self.ncirc)(*nq), self._gates, (c_size_t * self.ncirc)(*gcount),
+            (c_int32 * len(pidx))(*pidx), (c_size_t * self.ncirc)(*pcount), arr_t,
+            (c_size_t * self.ncirc)(*tcount), byref(o), byref(self.h)))
+
+    def run(self):
+        """(expvals[ncirc], [grad of circuit c], drift[ncirc])."""
+        ev = np.zeros(self.ncirc)
+        g = np.zeros(max(1, self.nparams))
+        dr = np.zeros(self.ncirc)
+        check(self._lib.qk_batch_run(self.h, ev.ctypes.data_as(POINTER(c_double)), g.ctypes.data_as(POINTER(c_double)),
+                                     dr.ctypes.data_as(POINTER(c_double))))
+        grads, k = [], 0
+        for n in self.param_counts:
+            grads.append(g[k:k + n].copy())
+            k += n
+        return ev, grads, dr
+
+    def set_params(self, params_per_circuit) -> None:
+        flat = np.concatenate([np.asarray(p, dtype=np.float64) for p in params_per_circuit])
+        check(self._lib.qk_batch_set_params(self.h, flat.ctypes.data_as(POINTER(c_double))))
+
+    def stats(self):
+        v = [c_int() for _ in range(6)]
+        check(self._lib.qk_batch_stats(self.h, *[byref(x) for x in v]))
+        k = ["steps", "launches", "tile_bits", "reg_bits", "adj_tile_bits", "adj_reg_bits"]
+        return {a: b.value for a, b in zip(k, v)}
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.qk_batch_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def apply_gates_dev(ptr: int, nqubits: int, dtype, circuit: Circuit, stream_ptr: int | None = None) -> None:
     """Per-gate path on caller-owned device memory (e.g. a torch tensor)."""
     check(_lib.load().qk_apply_gates_dev(c_void_p(ptr), int(nqubits), DTYPES[dtype], circuit.gates,
