@@ -196,7 +196,12 @@ typedef struct qk_plan_opts {
                              complex128, 13 for complex64; at most 14)      */
     int32_t reg_bits;     /* qubits held in registers per thread (default 3
                              for complex128, 4 for complex64; at most 5)    */
-    int32_t reserved[5];
+    int32_t fuse_width;   /* 0: register passes.  6: gates fused into dense
+                             6-qubit unitaries (FP64 on the host), each
+                             applied as a 64 x 64 complex contraction on the
+                             tensor cores in split precision (3 x BF16, FP32
+                             accumulate); complex64 states of >= 12 qubits */
+    int32_t reserved[4];
 } qk_plan_opts;
 
 typedef struct qk_plan qk_plan;
@@ -214,6 +219,11 @@ int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size
                           const qk_plan_opts *opts, qk_plan **out);
 /* Number of passes, program operations and register re-mappings. */
 int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t *remaps);
+/* Block k of a fuse_width = 6 plan (host data): its six qubits ascending
+ * (local index bit b = qubits[b]) and its 64 x 64 unitary, row-major complex
+ * (re, im) in u[2 * 64 * 64]; *is_perm = 1 for a VSWAP kept as a permutation
+ * (qubits then holds its targets, unused entries -1). */
+int qk_plan_dense_block(const qk_plan *p, size_t k, int32_t *qubits, double *u, int *is_perm);
 /* Run a plan on a state (same qubit count and dtype).  The first call copies
  * the plan's programs to the device (owned by the plan). */
 int qk_plan_apply(qk_sv *sv, qk_plan *p);

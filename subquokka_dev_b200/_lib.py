@@ -57,7 +57,8 @@ class QkConfig(ctypes.Structure):
 
 
 class QkPlanOpts(ctypes.Structure):
-    _fields_ = [("dtype", c_int32), ("tile_bits", c_int32), ("reg_bits", c_int32), ("reserved", c_int32 * 5)]
+    _fields_ = [("dtype", c_int32), ("tile_bits", c_int32), ("reg_bits", c_int32), ("fuse_width", c_int32),
+                ("reserved", c_int32 * 4)]
 
 
 class QkPauliTerm(ctypes.Structure):
@@ -108,6 +109,7 @@ PROTOTYPES = {
                                       POINTER(c_void_p)]),
     "qk_plan_stats": (c_int, [c_void_p, POINTER(c_size_t), POINTER(c_size_t), POINTER(c_size_t)]),
     "qk_plan_apply": (c_int, [c_void_p, c_void_p]),
+    "qk_plan_dense_block": (c_int, [c_void_p, c_size_t, POINTER(c_int32), POINTER(c_double), POINTER(c_int)]),
     "qk_plan_destroy": (None, [c_void_p]),
     "qk_apply_fused_noalloc": (c_int, [c_void_p, c_int, c_int, POINTER(QkGate), c_size_t, c_void_p]),
     "qk_expval_pauli": (c_int, [c_void_p, POINTER(QkPauliTerm), c_size_t, POINTER(c_double)]),

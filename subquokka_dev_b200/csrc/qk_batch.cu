@@ -12,9 +12,12 @@
 //
 // The reference has no counterpart (no gradients, no batching).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -237,34 +240,38 @@ struct qk_batch {
     cudaGraphExec_t exec = nullptr;
     size_t launches = 0;
 
-    void free_device() {
-        for (void *p : psi) if (p) cudaFree(p);
-        for (void *p : lam) if (p) cudaFree(p);
-        psi.clear();
-        lam.clear();
+    // programs, step tables, coefficient buffer and graph (rebuilt per tile shape)
+    void free_plans() {
         fdev.release();
         bdev.release();
         for (void *p : d_tables) cudaFree(p);
         d_tables.clear();
+        if (coef_host) cudaFreeHost(coef_host);
+        coef_host = nullptr;
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        steps.clear();
+    }
+    void free_device() {
+        free_plans();
+        for (void *p : psi) if (p) cudaFree(p);
+        for (void *p : lam) if (p) cudaFree(p);
+        psi.clear();
+        lam.clear();
         if (d_out) cudaFree(d_out);
         if (d_states) cudaFree(d_states);
         if (d_terms) cudaFree(d_terms);
         if (d_blk_circ) cudaFree(d_blk_circ);
         if (d_blk_first) cudaFree(d_blk_first);
-        if (coef_host) cudaFreeHost(coef_host);
         if (h_out) cudaFreeHost(h_out);
         d_out = nullptr;
         d_states = nullptr;
         d_terms = nullptr;
         d_blk_circ = nullptr;
         d_blk_first = nullptr;
-        coef_host = nullptr;
         h_out = nullptr;
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
-        steps.clear();
     }
     ~qk_batch() {
         free_device();
@@ -440,22 +447,45 @@ static int enqueue(qk_batch *b) {
     return QK_OK;
 }
 
-// Build plans, upload everything, capture the graph.
-static int prepare(qk_batch *b) {
-    b->free_device();
-    const int dt = b->dtype;
-    const size_t cs = dt == QK_C128 ? 16 : 8;
+// Build every circuit's plans (host threads, one circuit at a time each).
+static int build_all_plans(qk_batch *b) {
     b->fplan.assign(b->ncirc, HostPlan());
     b->bplan.assign(b->ncirc, HostPlan());
-    for (int c = 0; c < b->ncirc; ++c) {
-        PlanOptions fo = b->fo, bo = b->bo;
-        fo.tile_bits = std::min(fo.tile_bits, b->n[c]);
-        bo.tile_bits = std::min(bo.tile_bits, b->n[c]);
-        int rc = build_plan(b->gates[c].data(), b->gates[c].size(), b->n[c], fo, b->fplan[c]);
-        if (!rc)
-            rc = build_adjoint_plan(b->gates[c].data(), b->gates[c].size(), b->pidx[c].data(), b->n[c], bo, b->bplan[c]);
-        if (rc) return rc;
-    }
+    std::vector<int> rcs(b->ncirc, QK_OK);
+    std::vector<std::string> errs(b->ncirc);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int c = next++; c < b->ncirc; c = next++) {
+            PlanOptions fo = b->fo, bo = b->bo;
+            fo.tile_bits = std::min(fo.tile_bits, b->n[c]);
+            bo.tile_bits = std::min(bo.tile_bits, b->n[c]);
+            int rc = build_plan(b->gates[c].data(), b->gates[c].size(), b->n[c], fo, b->fplan[c]);
+            if (!rc)
+                rc = build_adjoint_plan(b->gates[c].data(), b->gates[c].size(), b->pidx[c].data(), b->n[c], bo,
+                                        b->bplan[c]);
+            if (rc) {
+                rcs[c] = rc;
+                errs[c] = qk_last_error();
+            }
+        }
+    };
+    const int nt = std::max(1, std::min<int>(b->ncirc, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    for (int c = 0; c < b->ncirc; ++c)
+        if (rcs[c]) return fail(rcs[c], "circuit %d: %s", c, errs[c].c_str());
+    return QK_OK;
+}
+
+// Build plans, upload programs and coefficients (states are allocated once).
+static int prepare(qk_batch *b) {
+    b->free_plans();
+    const int dt = b->dtype;
+    const size_t cs = dt == QK_C128 ? 16 : 8;
+    int prc = build_all_plans(b);
+    if (prc) return prc;
     // concatenate programs
     HostPlan fall, ball;
     b->f_op0.assign(b->ncirc, 0);
@@ -497,6 +527,7 @@ static int prepare(qk_batch *b) {
     e = cudaMallocHost(&b->coef_host, b->fcoef_bytes + b->bcoef_bytes);
     if (e != cudaSuccess) return cuda_err(e, "cudaMallocHost(coefficients)");
     fill_coefficients(b);
+    if (!b->psi.empty()) return QK_OK;
     // states, outputs
     b->psi.assign(b->ncirc, nullptr);
     b->lam.assign(b->ncirc, nullptr);
@@ -577,9 +608,10 @@ static int capture(qk_batch *b) {
 namespace {
 
 int full_prepare(qk_batch *b, const qk_batch_host_terms &ht) {
+    const bool first = b->psi.empty();
     int rc = prepare(b);
     if (!rc) rc = b->dtype == QK_C128 ? build_tables<double2>(b) : build_tables<float2>(b);
-    if (!rc) rc = upload_elem_tables(b, ht);
+    if (!rc && first) rc = upload_elem_tables(b, ht);
     if (!rc) rc = capture(b);
     return rc;
 }
@@ -668,9 +700,9 @@ int qk_batch_create(int ncirc, const int32_t *nqubits, const qk_gate *gates, con
     if (opts && opts->autotune) {
         // try tile shapes on the real batch, keep the fastest forward and adjoint
         struct Cand { int T, r; };
-        const std::vector<Cand> fc = b->dtype == QK_C64 ? std::vector<Cand>{{12, 3}, {13, 4}, {12, 4}, {11, 3}}
-                                                        : std::vector<Cand>{{12, 3}, {11, 3}, {11, 2}};
-        const std::vector<Cand> bc = b->dtype == QK_C64 ? std::vector<Cand>{{12, 3}, {11, 3}, {11, 2}, {12, 2}}
+        const std::vector<Cand> fc = b->dtype == QK_C64 ? std::vector<Cand>{{12, 3}, {12, 4}, {13, 4}}
+                                                        : std::vector<Cand>{{12, 3}, {11, 3}};
+        const std::vector<Cand> bc = b->dtype == QK_C64 ? std::vector<Cand>{{11, 3}, {12, 3}}
                                                         : std::vector<Cand>{{11, 2}, {10, 2}};
         float best = 1e30f;
         PlanOptions bf = b->fo, bb = b->bo;
@@ -719,19 +751,16 @@ int qk_batch_set_params(qk_batch *b, const double *params) {
         for (size_t i = 0; i < b->gates[c].size(); ++i)
             if (b->pidx[c][i] >= 0) b->gates[c][i].param = params[b->poff[c] + b->pidx[c][i]];
     // same gate structure -> same plans; only the coefficients change
+    std::vector<size_t> fsz(b->ncirc), bsz(b->ncirc);
     for (int c = 0; c < b->ncirc; ++c) {
-        HostPlan f, k;
-        int rc = build_plan(b->gates[c].data(), b->gates[c].size(), b->n[c],
-                            PlanOptions{b->fo.dtype, std::min(b->fo.tile_bits, b->n[c]), b->fo.reg_bits}, f);
-        if (!rc)
-            rc = build_adjoint_plan(b->gates[c].data(), b->gates[c].size(), b->pidx[c].data(), b->n[c],
-                                    PlanOptions{b->bo.dtype, std::min(b->bo.tile_bits, b->n[c]), b->bo.reg_bits}, k);
-        if (rc) return rc;
-        if (f.coef.size() != b->fplan[c].coef.size() || k.coef.size() != b->bplan[c].coef.size())
-            return fail(QK_ERR_ARG, "circuit %d: new parameters changed the plan", c);
-        b->fplan[c].coef.swap(f.coef);
-        b->bplan[c].coef.swap(k.coef);
+        fsz[c] = b->fplan[c].coef.size();
+        bsz[c] = b->bplan[c].coef.size();
     }
+    int rc = build_all_plans(b);
+    if (rc) return rc;
+    for (int c = 0; c < b->ncirc; ++c)
+        if (b->fplan[c].coef.size() != fsz[c] || b->bplan[c].coef.size() != bsz[c])
+            return fail(QK_ERR_ARG, "circuit %d: new parameters changed the plan", c);
     // the graph reads the pinned buffer when it runs: wait for a run in flight
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return cuda_err(e, "batch sync");

@@ -127,6 +127,20 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
                      HostPlan &plan);
 PlanOptions default_plan_options(int dtype, int n);
+
+// Dense fused blocks: consecutive gates on at most kDenseQubits qubits
+// multiplied (FP64, host) into one 2^k x 2^k unitary, applied as a
+// tensor-core contraction.  A block with perm != 0 is a VSWAP instead.
+constexpr int kDenseQubits = 6;
+constexpr int kDenseDim = 1 << kDenseQubits;
+struct DenseBlock {
+    int q[kDenseQubits];               // block qubits, ascending; local bit b = q[b]
+    std::vector<double> u;             // 64 x 64 complex, row-major, (re, im)
+    int perm = 0;                      // VSWAP: the Op below instead of u
+    Op perm_op;
+    int ngates = 0;
+};
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, std::vector<DenseBlock> &blocks);
 // Backward sweep of an adjoint gradient: the inverses of gates[ng-1..0] on
 // (psi, lambda), with the gradient of trainable gates (pidx[i] >= 0) taken
 // just before their inverse.

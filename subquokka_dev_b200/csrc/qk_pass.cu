@@ -313,10 +313,22 @@ int run_plan_at(void *state, int dtype, const HostPlan &hp, const TOp *ops, cons
 
 using namespace qk;
 
+namespace qk {
+struct DenseDesc;
+void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out);
+int run_dense_blocks(void *state, int n, const std::vector<DenseBlock> &blocks, const uint16_t *dA, int *derr,
+                     cudaStream_t st);
+}  // namespace qk
+
 struct qk_plan {
     HostPlan hp;
     DevPlan dp;
     bool uploaded = false;
+    // fuse_width = 6: dense blocks on the tensor cores instead of passes
+    bool dense = false;
+    std::vector<DenseBlock> blocks;
+    uint16_t *dA = nullptr;
+    int *derr = nullptr;
 };
 
 // Per-state scratch for the subcircuit path (one uploaded group plan).
@@ -361,6 +373,23 @@ int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_op
     if (!out || (!gates && n)) return fail(QK_ERR_ARG, "null argument");
     if (nqubits < 1 || nqubits > 36) return fail(QK_ERR_ARG, "nqubits must be in [1, 36], got %d", nqubits);
     const int dtype = opts ? opts->dtype : QK_C128;
+    if (opts && opts->fuse_width) {
+        if (opts->fuse_width != kDenseQubits) return fail(QK_ERR_ARG, "fuse_width must be 0 or %d", kDenseQubits);
+        if (dtype != QK_C64) return fail(QK_ERR_UNSUPPORTED, "tensor-core dense blocks run on complex64 states");
+        if (nqubits < 12) return fail(QK_ERR_UNSUPPORTED, "tensor-core dense blocks need at least 12 qubits");
+        auto *p = new qk_plan();
+        p->dense = true;
+        p->hp.n = nqubits;
+        p->hp.dtype = dtype;
+        int rc = build_dense_blocks(gates, n, nqubits, p->blocks);
+        if (rc) {
+            delete p;
+            return rc;
+        }
+        p->hp.ngates = n;
+        *out = p;
+        return QK_OK;
+    }
     PlanOptions o = default_plan_options(dtype, nqubits);
     if (opts && opts->tile_bits) o.tile_bits = opts->tile_bits;
     if (opts && opts->reg_bits) o.reg_bits = opts->reg_bits;
@@ -394,6 +423,12 @@ int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size
 
 int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t *remaps) {
     if (!p) return fail(QK_ERR_ARG, "null plan");
+    if (p->dense) {
+        if (passes) *passes = p->blocks.size();
+        if (program_ops) *program_ops = p->hp.ngates;
+        if (remaps) *remaps = 0;
+        return QK_OK;
+    }
     if (passes) *passes = p->hp.passes.size();
     if (program_ops) *program_ops = p->hp.ops.size();
     if (remaps) *remaps = p->hp.nremaps;
@@ -405,6 +440,33 @@ int qk_plan_apply(qk_sv *sv, qk_plan *p) {
     if (state_qubits(sv) != p->hp.n || state_dtype(sv) != p->hp.dtype)
         return fail(QK_ERR_ARG, "plan built for %d qubits dtype %d, state has %d qubits dtype %d", p->hp.n,
                     p->hp.dtype, state_qubits(sv), state_dtype(sv));
+    if (p->dense) {
+        cudaStream_t st = state_stream(sv);
+        if (!p->uploaded) {
+            std::vector<uint16_t> all, one;
+            for (const auto &b : p->blocks) {
+                if (b.perm) one.assign(2 * 128 * 128, 0);
+                else dense_block_operand(b, one);
+                all.insert(all.end(), one.begin(), one.end());
+            }
+            cudaError_t e = cudaMalloc(&p->dA, std::max<size_t>(1, all.size()) * sizeof(uint16_t));
+            if (e == cudaSuccess) e = cudaMalloc(&p->derr, sizeof(int));
+            if (e == cudaSuccess && !all.empty())
+                e = cudaMemcpy(p->dA, all.data(), all.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return cuda_err(e, "upload dense blocks");
+            p->uploaded = true;
+        }
+        cudaError_t e = cudaMemsetAsync(p->derr, 0, sizeof(int), st);
+        if (e != cudaSuccess) return cuda_err(e, "reset error flag");
+        int rc = run_dense_blocks(state_ptr(sv), p->hp.n, p->blocks, p->dA, p->derr, st);
+        if (rc) return rc;
+        int herr = 0;
+        e = cudaMemcpyAsync(&herr, p->derr, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_err(e, "dense blocks");
+        if (herr) return fail(QK_ERR_CUDA, "a tensor-core pass gave up waiting for its contraction");
+        return QK_OK;
+    }
     if (!p->uploaded) {
         int rc = upload_plan(p->hp, p->hp.dtype, p->dp, state_stream(sv));
         if (rc) return rc;
@@ -415,8 +477,26 @@ int qk_plan_apply(qk_sv *sv, qk_plan *p) {
     return run_plan(state_ptr(sv), p->hp.dtype, p->hp, p->dp, state_stream(sv));
 }
 
+int qk_plan_dense_block(const qk_plan *p, size_t k, int32_t *qubits, double *u, int *is_perm) {
+    if (!p || !qubits || !u || !is_perm) return fail(QK_ERR_ARG, "null argument");
+    if (!p->dense) return fail(QK_ERR_ARG, "not a dense plan");
+    if (k >= p->blocks.size()) return fail(QK_ERR_ARG, "block %zu of %zu", k, p->blocks.size());
+    const DenseBlock &b = p->blocks[k];
+    *is_perm = b.perm;
+    if (b.perm) {
+        for (int i = 0; i < kDenseQubits; ++i) qubits[i] = -1;
+        for (int i = 0; i < b.perm_op.nq && i < kDenseQubits; ++i) qubits[i] = b.perm_op.q[i];
+        return QK_OK;
+    }
+    for (int i = 0; i < kDenseQubits; ++i) qubits[i] = b.q[i];
+    std::memcpy(u, b.u.data(), b.u.size() * sizeof(double));
+    return QK_OK;
+}
+
 void qk_plan_destroy(qk_plan *p) {
     if (!p) return;
+    if (p->dA) cudaFree(p->dA);
+    if (p->derr) cudaFree(p->derr);
     p->dp.release();
     delete p;
 }

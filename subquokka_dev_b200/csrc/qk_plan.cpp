@@ -435,6 +435,116 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
     return b.greedy(0, ops.size());
 }
 
+// Apply a lowered op (dense matrix over its targets, little-endian) to the
+// 64 columns of a 6-qubit block unitary in place; loc[k] = local bit of op.q[k].
+static void block_apply(std::vector<double> &u, const Op &op, const int *loc) {
+    const int nq = op.nq, d = 1 << nq;
+    double m[2 * 16 * 16];
+    std::memset(m, 0, sizeof m);
+    auto put = [&](int r, int c, double re, double im) { m[2 * (r * d + c)] = re; m[2 * (r * d + c) + 1] = im; };
+    switch (op.kind) {
+    case OP_DENSE1: case OP_DENSE2:
+        for (int k = 0; k < d * d; ++k) put(k / d, k % d, op.m[2 * k], op.m[2 * k + 1]);
+        break;
+    case OP_PHASE1: put(0, 0, 1, 0); put(1, 1, op.m[0], op.m[1]); break;
+    case OP_DIAG1: put(0, 0, op.m[0], op.m[1]); put(1, 1, op.m[2], op.m[3]); break;
+    case OP_PHASE2: for (int k = 0; k < 3; ++k) put(k, k, 1, 0); put(3, 3, op.m[0], op.m[1]); break;
+    case OP_DIAG2: for (int k = 0; k < 4; ++k) put(k, k, op.m[2 * k], op.m[2 * k + 1]); break;
+    case OP_SWAP2: put(0, 0, 1, 0); put(1, 2, 1, 0); put(2, 1, 1, 0); put(3, 3, 1, 0); break;
+    default: return;
+    }
+    int mask = 0;
+    for (int k = 0; k < nq; ++k) mask |= 1 << loc[k];
+    for (int col = 0; col < kDenseDim; ++col) {
+        double *v = u.data() + 2 * col;  // column col: element (row r) at 2 * (r * 64 + col)
+        for (int base = 0; base < kDenseDim; ++base) {
+            if (base & mask) continue;
+            int idx[16];
+            double xr[16], xi[16];
+            for (int s = 0; s < d; ++s) {
+                int r = base;
+                for (int k = 0; k < nq; ++k)
+                    if ((s >> k) & 1) r |= 1 << loc[k];
+                idx[s] = r;
+                xr[s] = v[2 * r * kDenseDim];
+                xi[s] = v[2 * r * kDenseDim + 1];
+            }
+            for (int r = 0; r < d; ++r) {
+                double yr = 0, yi = 0;
+                for (int c = 0; c < d; ++c) {
+                    const double ar = m[2 * (r * d + c)], ai = m[2 * (r * d + c) + 1];
+                    yr += ar * xr[c] - ai * xi[c];
+                    yi += ar * xi[c] + ai * xr[c];
+                }
+                v[2 * idx[r] * kDenseDim] = yr;
+                v[2 * idx[r] * kDenseDim + 1] = yi;
+            }
+        }
+    }
+}
+
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, std::vector<DenseBlock> &blocks) {
+    if (n < kDenseQubits) return fail(QK_ERR_ARG, "dense blocks need at least %d qubits", kDenseQubits);
+    std::vector<Op> ops;
+    int rc = lower_all(gates, ng, n, ops);
+    if (rc) return rc;
+    blocks.clear();
+    std::vector<size_t> pending(ops.size());
+    for (size_t i = 0; i < ops.size(); ++i) pending[i] = i;
+    while (!pending.empty()) {
+        if (ops[pending[0]].kind == OP_PERM) {
+            DenseBlock b;
+            b.perm = 1;
+            b.perm_op = ops[pending[0]];
+            b.ngates = 1;
+            blocks.push_back(std::move(b));
+            pending.erase(pending.begin());
+            continue;
+        }
+        // greedy: gates join while the union of qubits stays within 6 and no
+        // earlier gate on their qubits was left out
+        std::vector<int> Q;
+        std::vector<char> blocked(n, 0);
+        std::vector<size_t> take, rest;
+        for (size_t i : pending) {
+            const Op &op = ops[i];
+            bool ok = op.kind != OP_PERM;
+            for (int k = 0; k < op.nq && ok; ++k) ok = !blocked[op.q[k]];
+            if (ok) {
+                int need = 0;
+                for (int k = 0; k < op.nq; ++k)
+                    if (std::find(Q.begin(), Q.end(), op.q[k]) == Q.end()) ++need;
+                ok = (int)Q.size() + need <= kDenseQubits;
+                if (ok)
+                    for (int k = 0; k < op.nq; ++k)
+                        if (std::find(Q.begin(), Q.end(), op.q[k]) == Q.end()) Q.push_back(op.q[k]);
+            }
+            if (ok) take.push_back(i);
+            else {
+                for (int k = 0; k < op.nq; ++k) blocked[op.q[k]] = 1;
+                rest.push_back(i);
+            }
+        }
+        for (int q = 0; q < n && (int)Q.size() < kDenseQubits; ++q)
+            if (std::find(Q.begin(), Q.end(), q) == Q.end()) Q.push_back(q);
+        std::sort(Q.begin(), Q.end());
+        DenseBlock b;
+        for (int k = 0; k < kDenseQubits; ++k) b.q[k] = Q[k];
+        b.u.assign(2 * kDenseDim * kDenseDim, 0.0);
+        for (int k = 0; k < kDenseDim; ++k) b.u[2 * (k * kDenseDim + k)] = 1.0;
+        for (size_t i : take) {
+            int loc[QK_MAX_TARGETS];
+            for (int k = 0; k < ops[i].nq; ++k)
+                loc[k] = (int)(std::find(Q.begin(), Q.end(), ops[i].q[k]) - Q.begin());
+            block_apply(b.u, ops[i], loc);
+        }
+        b.ngates = (int)take.size();
+        blocks.push_back(std::move(b));
+        pending.swap(rest);
+    }
+    return QK_OK;
+}
+
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
                      HostPlan &plan) {
     int rc = check_options(o, n);

@@ -239,12 +239,13 @@ class Plan:
     the state (qk_plan_create / qk_plan_create_groups)."""
 
     def __init__(self, circuit: Circuit, nqubits: int, dtype="c128", tile_bits: int = 0, reg_bits: int = 0,
-                 groups: bool = False):
+                 groups: bool = False, fuse_width: int = 0):
         self._lib = _lib.load()
         o = _lib.QkPlanOpts()
         o.dtype = DTYPES[dtype]
         o.tile_bits = int(tile_bits)
         o.reg_bits = int(reg_bits)
+        o.fuse_width = int(fuse_width)
         self.h = c_void_p()
         if groups:
             check(self._lib.qk_plan_create_groups(circuit.gates, circuit.group_sizes, circuit.ngroups, int(nqubits),
@@ -262,6 +263,15 @@ class Plan:
 
     def apply(self, sv: "StateVector") -> None:
         check(self._lib.qk_plan_apply(sv.h, self.h))
+
+    def dense_block(self, k: int):
+        """(qubits, 64 x 64 unitary or None, is_perm) of block k of a fuse_width = 6 plan."""
+        qs = (c_int32 * 6)()
+        u = np.zeros(2 * 64 * 64)
+        perm = c_int()
+        check(self._lib.qk_plan_dense_block(self.h, int(k), qs, u.ctypes.data_as(POINTER(c_double)), byref(perm)))
+        qlist = [q for q in qs if q >= 0]
+        return qlist, (None if perm.value else u.view(np.complex128).reshape(64, 64)), bool(perm.value)
 
     def close(self) -> None:
         if self.h:

@@ -18,8 +18,8 @@ def zero(n):
     return s
 
 
-def run_plan(n, circ, init, dtype="c128", tile=0, reg=0, groups=False):
-    plan = Plan(circ, n, dtype, tile, reg, groups)
+def run_plan(n, circ, init, dtype="c128", tile=0, reg=0, groups=False, fuse_width=0):
+    plan = Plan(circ, n, dtype, tile, reg, groups, fuse_width)
     with StateVector(n, dtype) as sv:
         if init is not None:
             sv.upload(init)
@@ -118,3 +118,28 @@ def test_plan_reuse_and_large_state():
         b.apply(circ)
         x, y = a.download(), b.download()
     assert np.abs(x - y).max() <= 1e-12
+
+
+def fidelity_err(out, ref):
+    ov = np.vdot(ref, out)
+    return 1 - abs(ov) ** 2 / (np.vdot(ref, ref).real * np.vdot(out, out).real)
+
+
+@pytest.mark.parametrize("n", [12, 14, 17])
+def test_tensor_core_dense_blocks(n):
+    # 6-qubit blocks as 64 x 64 complex contractions on tcgen05 (3 x BF16,
+    # FP32 accumulate): 1 - F <= 1e-6 against the FP64 oracle
+    circ = random_circuit(n, 200, 300 + n)
+    init = circuits.random_state(n, 31)
+    ref = oracle.apply_circuit(init, n, circ)
+    out = run_plan(n, circ, init, "c64", fuse_width=6)
+    assert fidelity_err(out, ref) <= 1e-6
+    assert np.abs(out - ref).max() <= 5e-5
+
+
+def test_tensor_core_random_circuit_family():
+    n = 20
+    circ = circuits.random_u3_cz(n, 8, 40)
+    ref = oracle.apply_circuit(zero(n), n, circ)
+    out = run_plan(n, circ, None, "c64", fuse_width=6)
+    assert fidelity_err(out, ref) <= 1e-6

@@ -1,4 +1,5 @@
 """Host side of the fused planner (no GPU): pass counts and option checks."""
+import numpy as np
 import pytest
 
 import subquokka_dev_b200 as sq
@@ -47,3 +48,40 @@ def test_plan_rejects_bad_qubits():
     c = Circuit([make_gate("H", [20])])
     with pytest.raises(sq.QkError):
         Plan(c, 10, "c128")
+
+
+def apply_block(state, n, qubits, u):
+    """numpy: apply a 64 x 64 unitary on the given six qubits (local bit b = qubits[b])."""
+    psi = state.reshape([2] * n)  # axis n-1-q is qubit q
+    axes = [n - 1 - q for q in reversed(qubits)]  # block index bit b = qubit qubits[b]: most significant first
+    t = np.moveaxis(psi, axes, list(range(6))).reshape(64, -1)
+    t = u @ t
+    return np.moveaxis(t.reshape([2] * 6 + [2] * (n - 6)), list(range(6)), axes).reshape(-1)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_dense_fuser_blocks_reproduce_the_circuit(seed):
+    import oracle
+    from test_gpu_fused import random_circuit
+    n = 12
+    circ = random_circuit(n, 150, seed)
+    p = Plan(circ, n, "c64", fuse_width=6)
+    nb = p.stats()[0]
+    s = circuits.random_state(n, seed)
+    out = s.copy()
+    for k in range(nb):
+        qs, u, perm = p.dense_block(k)
+        if perm:
+            out = oracle.apply_circuit(out, n, Circuit([make_gate("VSWAP", qs)]))
+        else:
+            assert np.allclose(u.conj().T @ u, np.eye(64), atol=1e-12)
+            out = apply_block(out, n, qs, u)
+    assert np.abs(out - oracle.apply_circuit(s, n, circ)).max() < 1e-12
+
+
+def test_dense_fuser_block_count():
+    c = circuits.random_u3_cz(33, 24, 33)
+    nb = Plan(c, 33, "c64", fuse_width=6).stats()[0]
+    assert nb < c.ngates / 4
+    with pytest.raises(sq.QkError):
+        Plan(c, 33, "c128", fuse_width=6)
