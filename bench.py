@@ -243,8 +243,8 @@ def fused_variants(args, circ, exact, plain_ms, alg):
     from subquokka_dev_b200 import Plan, StateVector
     out = {}
     n = args.qubits
-    for dtype in ("c128", "c64"):
-        plan = Plan(circ, n, dtype)
+    for key, dtype, fw in (("c128", "c128", 0), ("c64", "c64", 0), ("c64_tensor_core", "c64", 6)):
+        plan = Plan(circ, n, dtype, fuse_width=fw)
         passes, ops, remaps = plan.stats()
         sv = StateVector(n, dtype)
         sv.set_stream(torch.cuda.current_stream().cuda_stream)
@@ -255,7 +255,7 @@ def fused_variants(args, circ, exact, plain_ms, alg):
         ms = time_device(run, 2, max(1, args.steps))
         dmax, infid = compare_states(sv, exact)
         amp = 16 if dtype == "c128" else 8
-        out[dtype] = {"ms_per_circuit": ms, "speedup_vs_plain_c128": plain_ms / ms, "passes": passes,
+        out[key] = {"ms_per_circuit": ms, "speedup_vs_plain_c128": plain_ms / ms, "passes": passes,
                       "program_ops": ops, "remaps": remaps,
                       "hbm_gbs_passes": passes * 2 * (amp << n) / (ms / 1e3) / 1e9,
                       "max_abs_damp_vs_c128": dmax, "one_minus_fidelity_vs_c128": infid}
@@ -322,31 +322,37 @@ def extra_workloads(args):
         res[key]["max_rel_grad_err_vs_c128_per_gate"] = float(np.abs(g - ref).max() / np.abs(ref).max())
     out["hea26_adjoint"] = res
 
-    # 33-qubit c64 fused; error at 28 qubits against complex128
+    # 33-qubit c64: width-6 dense blocks on the tensor cores (and the CUDA-core
+    # register passes for comparison); error at 28 qubits against complex128
     n33, l33 = 33, 24
     c33 = circuits.random_u3_cz(n33, l33, 33)
-    p33 = Plan(c33, n33, "c64")
+    res33 = {"qubits": n33, "layers": l33, "gates": c33.ngates, "state_bytes": 8 << n33}
     sv = StateVector(n33, "c64")
     sv.set_stream(stream)
+    for key, fw in (("tensor_core_width6", 6), ("cuda_core_passes", 0)):
+        p33 = Plan(c33, n33, "c64", fuse_width=fw)
 
-    def run33():
-        sv.reset()
-        p33.apply(sv)
-    ms33 = time_device(run33, 1, 2)
+        def run33():
+            sv.reset()
+            p33.apply(sv)
+        ms33 = time_device(run33, 1, 2)
+        np33 = p33.stats()[0]
+        res33[key] = {"ms_per_circuit": ms33, "passes": np33,
+                      "hbm_gbs_passes": np33 * 2 * (8 << n33) / (ms33 / 1e3) / 1e9}
+        p33.close()
     sv.close()
-    res33 = {"qubits": n33, "layers": l33, "gates": c33.ngates, "passes": p33.stats()[0], "ms_per_circuit": ms33,
-             "state_bytes": 8 << n33, "method": "fused passes, FP32 CUDA-core arithmetic"}
-    p33.close()
     c28 = circuits.random_u3_cz(28, l33, 33)
-    a, b = StateVector(28, "c128"), StateVector(28, "c64")
+    a = StateVector(28, "c128")
     a.apply(c28)
-    p28 = Plan(c28, 28, "c64")
-    p28.apply(b)
-    dmax, infid = compare_states(b, a)
-    res33.update({"check_qubits": 28, "max_abs_damp_vs_c128": dmax, "one_minus_fidelity_vs_c128": infid})
+    for key, fw in (("tensor_core_width6", 6), ("cuda_core_passes", 0)):
+        b = StateVector(28, "c64")
+        p28 = Plan(c28, 28, "c64", fuse_width=fw)
+        p28.apply(b)
+        dmax, infid = compare_states(b, a)
+        res33[key].update({"check_qubits": 28, "max_abs_damp_vs_c128": dmax, "one_minus_fidelity_vs_c128": infid})
+        b.close()
+        p28.close()
     a.close()
-    b.close()
-    p28.close()
     out["random33_c64"] = res33
 
     # batch of 256 variational circuits (14-22 qubits, 4-16 layers), complex64,

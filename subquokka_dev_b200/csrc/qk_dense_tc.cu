@@ -51,6 +51,11 @@ __host__ __device__ __forceinline__ uint32_t kmajor_off(uint32_t r, uint32_t k) 
 
 __device__ __forceinline__ uint32_t s_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Shared-memory position of tile element j: the 16-byte pair (j, j ^ 1) stays
+// together (cp.async granule); the pair index is XORed with a fold of the
+// higher index bits so that strided block-qubit accesses spread over banks.
+__device__ __forceinline__ uint32_t tcz(uint32_t j) { return j ^ ((((j >> 4) ^ (j >> 7) ^ (j >> 10)) & 7u) << 1); }
+
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
     d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;   // leading byte offset: next K chunk
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const uint32_t j = 2 * (tid + 256 * u);
-            const uint32_t dst = s_u32(buf + j);
+            const uint32_t dst = s_u32(buf + tcz(j));
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(s + (base | goff(u))) : "memory");
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -156,7 +161,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
                 float hi[8], lo[8];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const float2 x = tl[jb[i0 + 4 * c + q] | jo[n]];
+                    const float2 x = tl[tcz(jb[i0 + 4 * c + q] | jo[n])];
                     const float xs[2] = {x.x, x.y};
 #pragma unroll
                     for (int b = 0; b < 2; ++b) {
@@ -225,14 +230,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
             const uint32_t m = (uint32_t)(warp & 3) * 32u + lane, ip = m >> 1, comp = m & 1;
             const uint32_t n0 = 32u * (uint32_t)(warp >> 2);
 #pragma unroll
-            for (int q = 0; q < 32; ++q) reinterpret_cast<float *>(&tl[jb[ip] | jo[n0 + q]])[comp] = __uint_as_float(r[q]);
+            for (int q = 0; q < 32; ++q)
+                reinterpret_cast<float *>(&tl[tcz(jb[ip] | jo[n0 + q])])[comp] = __uint_as_float(r[q]);
         }
         tc_fence_before();
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const uint32_t j = 2 * (tid + 256 * u);
-            *reinterpret_cast<float4 *>(s + (base | goff(u))) = *reinterpret_cast<const float4 *>(tl + j);
+            *reinterpret_cast<float4 *>(s + (base | goff(u))) = *reinterpret_cast<const float4 *>(tl + tcz(j));
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
