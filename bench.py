@@ -205,6 +205,22 @@ def kernel_class(g):
     return f"kind{g.kind}"
 
 
+def max_over_ranks(value: float, world: int, device="cuda") -> float:
+    """The max of a per-rank number over all ranks (the slowest replica)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, bytes_per_step: int, steps: int, max_ms: float) -> float:
+    """Whole-job GB/s: every rank runs its own replica, timed by the slowest."""
+    return world * bytes_per_step * steps / (max_ms / 1e3) / 1e9
+
+
 def time_device(fn, warmup, steps):
     """Device time (ms) per call of fn, CUDA events on the current stream."""
     import torch
@@ -442,13 +458,9 @@ def our_arm(args, rank, world):
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
-    total_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     ms_per_step = total_ms / args.steps
-    value = world * alg * args.steps / (total_ms / 1e3) / 1e9
+    value = replica_throughput(world, alg, args.steps, total_ms)
 
     # dominant kernel: the dense one-qubit sweep on a high qubit (U1, 2S bytes)
     peak, peak_kind = measured_peak_hbm()
@@ -488,11 +500,7 @@ def our_arm(args, rank, world):
             sv.reset()
             sv.apply(circ)
             check(lib.qk_sv_download(sv.h, hp))
-        el = time.perf_counter() - t0
-        tt = torch.tensor([el], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        el = float(tt.item())
+        el = max_over_ranks(time.perf_counter() - t0, world)
         import ctypes as _ct
         e2e = {"value": world * alg * e2e_steps / el / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": _ct.sizeof(circ.gates._type_) * circ.ngates,
