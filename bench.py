@@ -336,6 +336,21 @@ def extra_workloads(args):
     for k, g in grads.items():
         key = f"{k[0]}_{'fused' if k[1] else 'per_gate'}"
         res[key]["max_rel_grad_err_vs_c128_per_gate"] = float(np.abs(g - ref).max() / np.abs(ref).max())
+    if not args.no_cpu_baseline:
+        # the reference has no gradient code: this project's FP64 CPU adjoint
+        # restatement (OpenMP, all host cores) on the first layer of the same ansatz
+        import oracle
+        pc1 = hea_template(n, 1)
+        c1, i1 = pc1.bind(params[:pc1.nparams])
+        z = np.zeros(1 << n, np.complex128)
+        z[0] = 1
+        t0 = time.perf_counter()
+        oracle.adjoint_grad(z, n, c1, i1, pc1.nparams, terms)
+        secs = time.perf_counter() - t0
+        res["cpu_baseline"] = {"grads_per_s": pc1.nparams / secs, "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"first layer ({pc1.nparams} parameters) of the 26-qubit ansatz, FP64 C "
+                                         "adjoint restatement (the reference computes no gradients)",
+                               "seconds": secs}
     out["hea26_adjoint"] = res
 
     # 33-qubit c64: width-6 dense blocks on the tensor cores (and the CUDA-core

@@ -95,7 +95,9 @@ typedef struct qk_config {
     int32_t MPI_testing;      /* MPI_testing, default 0                      */
     int32_t MPI_buffe_size;   /* MPI_buffe_size (sic), default 16            */
     int32_t precision;        /* precision=c128|c64 -> qk_dtype, default c128 */
-    int32_t fuse_width;       /* fuse_width, default 0: per-gate kernels     */
+    int32_t fuse_width;       /* fuse_width, default 0: per-gate kernels; on a
+                                 flat circuit > 0 runs fused passes, 6 with
+                                 precision=c64 tensor-core 6-qubit blocks    */
     int32_t dump_binary;      /* dump_format=bin -> 1, default 0 (text)      */
     char runner_type[32];     /* runner_type, default "IO"; "GPU" selects us */
     char dump_file[256];      /* dump_file, default ""                       */
@@ -327,8 +329,8 @@ void qk_batch_destroy(qk_batch *b);
 int qk_apply_fused_noalloc(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n, void *cuda_stream);
 
 /* Run a parsed circuit the way Simulator::run does (src/simulator.cpp:671-706):
- * groups if cfg->is_subcircuit, else gates; *seconds receives the device time
- * of the runner span alone. */
+ * groups if cfg->is_subcircuit, else gates (fused passes if cfg->fuse_width >
+ * 0); *seconds receives the device time of the runner span alone. */
 int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds);
 
 #ifdef __cplusplus

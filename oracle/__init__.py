@@ -47,6 +47,9 @@ def load():
         lib.qko_apply_list.restype = c_int
         lib.qko_expval_zz_x.argtypes = [POINTER(c_double), c_int, POINTER(c_double), POINTER(c_double)]
         lib.qko_expval_zz_x.restype = c_double
+        lib.qko_adjoint_grad.argtypes = [POINTER(c_double), c_int, POINTER(QkGate), c_size_t, POINTER(c_int), c_size_t,
+                                         ctypes.c_void_p, c_size_t, POINTER(c_double), POINTER(c_double)]
+        lib.qko_adjoint_grad.restype = c_int
         _lib = lib
     return _lib
 
@@ -141,3 +144,22 @@ def param_shift_grad(pc, params: np.ndarray, terms) -> np.ndarray:
             e = pauli_expval(apply_circuit(z0, n, circ), n, terms)
             grad[p] += sgn * e / 2
     return grad
+
+
+class _Term(ctypes.Structure):
+    _fields_ = [("coeff", c_double), ("x", ctypes.c_ulonglong), ("z", ctypes.c_ulonglong)]
+
+
+def adjoint_grad(state: np.ndarray, n: int, circuit, pidx, nparams: int, terms):
+    """FP64 CPU adjoint restatement: (<H>, gradient) after circuit on state."""
+    s = np.array(state, dtype=np.complex128, copy=True)
+    p = np.ascontiguousarray(pidx, dtype=np.int32)
+    tl = list(terms)
+    arr = (_Term * max(1, len(tl)))(*[_Term(float(c), int(x), int(z)) for c, x, z in tl])
+    g = np.zeros(max(1, nparams))
+    ev = c_double()
+    rc = load().qko_adjoint_grad(_dptr(s), n, circuit.gates, circuit.ngates, p.ctypes.data_as(POINTER(c_int)),
+                                 nparams, ctypes.cast(arr, ctypes.c_void_p), len(tl), ctypes.byref(ev), _dptr(g))
+    if rc:
+        raise RuntimeError("oracle adjoint: unsupported gate")
+    return ev.value, g[:nparams]

@@ -12,6 +12,7 @@
 
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 typedef struct { double re, im; } cx;
@@ -204,4 +205,89 @@ double qko_expval_zz_x(const double *s, int n, const double *J, const double *h)
         acc += h[i] * e;
     }
     return acc;
+}
+
+/* ---------------------------------------------------------------------------
+ * Adjoint gradient (the engine's own addition; the reference has none).
+ * psi = U_L..U_1 psi0, lambda = H psi, then for k = L..1:
+ *   g[p(k)] += Im <lambda|G_k|psi>,  psi <- U_k^-1 psi,  lambda <- U_k^dag lambda
+ * with U^-1 = U^dag (a gate with negated angle, or the conjugate transpose).
+ * ------------------------------------------------------------------------- */
+static int inverse_gate(const qk_gate *g, qk_gate *inv) {
+    *inv = *g;
+    switch (g->kind) {
+    case QK_GATE_H: case QK_GATE_X: case QK_GATE_Y: case QK_GATE_Z: case QK_GATE_SWAP:
+    case QK_GATE_VSWAP: case QK_GATE_MPI_VSWAP:
+        return 0;
+    case QK_GATE_P: case QK_GATE_RX: case QK_GATE_RY: case QK_GATE_RZ: case QK_GATE_CP: case QK_GATE_RZZ:
+        inv->param = -g->param;
+        return 0;
+    case QK_GATE_U1: case QK_GATE_U2: {
+        const int d = g->kind == QK_GATE_U1 ? 2 : 4;
+        for (int r = 0; r < d; ++r)
+            for (int c = 0; c < d; ++c) {
+                inv->coeff[2 * (r * d + c)] = g->coeff[2 * (c * d + r)];
+                inv->coeff[2 * (r * d + c) + 1] = -g->coeff[2 * (c * d + r) + 1];
+            }
+        return 0;
+    }
+    default:
+        return -1;
+    }
+}
+
+static void apply_terms(double *out, const double *psi, int n, const qko_term *t, size_t nt) {
+    const uint64_t N = 1ull << n;
+    memset(out, 0, sizeof(double) * 2 * N);
+    for (size_t k = 0; k < nt; ++k) {
+        const int ip = __builtin_popcountll(t[k].x & t[k].z) & 3;
+#pragma omp parallel for schedule(static)
+        for (uint64_t j = 0; j < N; ++j) {
+            const uint64_t src = j ^ t[k].x;
+            const double c = (__builtin_popcountll(src & t[k].z) & 1) ? -t[k].coeff : t[k].coeff;
+            const double fr = ip == 0 ? c : ip == 2 ? -c : 0, fi = ip == 1 ? c : ip == 3 ? -c : 0;
+            out[2 * j] += fr * psi[2 * src] - fi * psi[2 * src + 1];
+            out[2 * j + 1] += fr * psi[2 * src + 1] + fi * psi[2 * src];
+        }
+    }
+}
+
+int qko_adjoint_grad(double *psi, int n, const qk_gate *gates, size_t ng, const int *pidx, size_t nparams,
+                     const qko_term *terms, size_t nterms, double *expval, double *grad) {
+    const uint64_t N = 1ull << n;
+    if (qko_apply_list(psi, n, gates, ng)) return -1;
+    double *lam = (double *)malloc(sizeof(double) * 2 * N);
+    if (!lam) return -1;
+    apply_terms(lam, psi, n, terms, nterms);
+    double e = 0;
+#pragma omp parallel for reduction(+ : e) schedule(static)
+    for (uint64_t j = 0; j < N; ++j) e += psi[2 * j] * lam[2 * j] + psi[2 * j + 1] * lam[2 * j + 1];
+    *expval = e;
+    for (size_t p = 0; p < nparams; ++p) grad[p] = 0;
+    for (size_t k = ng; k-- > 0;) {
+        const qk_gate *g = &gates[k];
+        if (pidx && pidx[k] >= 0) {
+            const int gen = g->kind == QK_GATE_RX ? 1 : g->kind == QK_GATE_RY ? 2 : g->kind == QK_GATE_RZ ? 3 : 0;
+            if (!gen) { free(lam); return -1; }
+            const int t = g->q[0];
+            const uint64_t h = 1ull << t;
+            double s = 0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+            for (uint64_t p = 0; p < N / 2; ++p) {
+                const uint64_t i0 = ins0(p, t), i1 = i0 + h;
+                const cx a0 = ld(psi, i0), a1 = ld(psi, i1), l0 = ld(lam, i0), l1 = ld(lam, i1);
+                /* Im conj(l) a = l.re a.im - l.im a.re;  Re conj(l) a = l.re a.re + l.im a.im */
+                if (gen == 1) s += (l0.re * a1.im - l0.im * a1.re) + (l1.re * a0.im - l1.im * a0.re);
+                else if (gen == 2) s += (l1.re * a0.re + l1.im * a0.im) - (l0.re * a1.re + l0.im * a1.im);
+                else s += (l0.re * a0.im - l0.im * a0.re) - (l1.re * a1.im - l1.im * a1.re);
+            }
+            grad[pidx[k]] += s;
+        }
+        qk_gate inv;
+        if (inverse_gate(g, &inv)) { free(lam); return -1; }
+        qko_apply(psi, n, &inv);
+        qko_apply(lam, n, &inv);
+    }
+    free(lam);
+    return 0;
 }

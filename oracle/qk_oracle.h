@@ -31,6 +31,16 @@ int qko_apply_list(double *state, int n, const qk_gate *gates, size_t ng);
 /* <psi| H |psi> for H = sum_i J[i] Z_i Z_{i+1} (i < n-1) + sum_i h[i] X_i. */
 double qko_expval_zz_x(const double *state, int n, const double *J, const double *h);
 
+/* One Pauli string coeff * i^popcount(x & z) X^x Z^z (the engine's qk_pauli_term). */
+typedef struct { double coeff; unsigned long long x, z; } qko_term;
+
+/* FP64 adjoint gradient of <H> after gates[0..ng) applied to state (which is
+ * overwritten): gate i with pidx[i] >= 0 is trainable (RX, RY, RZ) and adds
+ * Im <lambda|G|psi> to grad[pidx[i]]; *expval receives <H>.  Returns 0, or -1
+ * for a gate this restatement cannot invert or differentiate. */
+int qko_adjoint_grad(double *state, int n, const qk_gate *gates, size_t ng, const int *pidx, size_t nparams,
+                     const qko_term *terms, size_t nterms, double *expval, double *grad);
+
 #ifdef __cplusplus
 }
 #endif

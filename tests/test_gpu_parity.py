@@ -200,3 +200,29 @@ def test_cli_text_dump_format(tmp_path):
     assert r.returncode == 0, r.stderr
     vals = (tmp_path / "res0.txt").read_text().split()
     assert len(vals) == 16 and vals[0] == "%.11f" % (0.70710678118 ** 3) and vals[1] == "0.00000000000"
+
+
+@pytest.mark.parametrize("precision,fuse_width,tol", [("c128", 1, 1e-12), ("c64", 1, 2e-6), ("c64", 6, 5e-5)])
+def test_cli_fused_forms(tmp_path, precision, fuse_width, tol):
+    n = 14
+    ini = tmp_path / "x.ini"
+    ini.write_text(f"[system]\ntotal_qbit={n}\nfile_qbit=2\nchunk_qbit=10\nrunner_type=GPU\nis_subcircuit=0\n"
+                   f"precision={precision}\nfuse_width={fuse_width}\ndump_file={tmp_path}/s.bin\ndump_format=bin\n")
+    circ = circuits.random_u3_cz(n, 6, 77)
+    cir = tmp_path / "c.txt"
+    cir.write_text(circ.to_text())
+    r = subprocess.run([CLI, "-i", str(ini), "-c", str(cir)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = np.fromfile(tmp_path / "s.bin", dtype=np.complex128)
+    z = np.zeros(1 << n, np.complex128)
+    z[0] = 1
+    assert np.abs(out - oracle.apply_circuit(z, n, circ)).max() <= tol
+
+
+def test_out_of_memory_is_an_error_not_a_fault():
+    from subquokka_dev_b200 import QkError
+    with pytest.raises(QkError) as e:
+        StateVector(36)                      # 1 TiB complex128
+    assert e.value.code == -7
+    with StateVector(10) as sv:              # the context is still usable
+        sv.apply(circuits.qft(10))

@@ -105,3 +105,19 @@ def test_parameter_shift_matches_finite_differences():
             v[p] += sg * eps
             e.append(oracle.pauli_expval(oracle.apply_circuit(z0, n, pc.bind(v)[0]), n, terms))
         assert abs((e[0] - e[1]) / (2 * eps) - ps[p]) < 1e-7
+
+
+def test_c_adjoint_restatement_matches_parameter_shift():
+    from subquokka_dev_b200 import zz_x_hamiltonian
+    from subquokka_dev_b200.torch_shim import hea_template
+    n, layers = 6, 3
+    pc = hea_template(n, layers)
+    rng = np.random.default_rng(8)
+    params = rng.uniform(-np.pi, np.pi, pc.nparams)
+    terms = zz_x_hamiltonian(n, rng.standard_normal(n - 1), rng.standard_normal(n)) + [(0.3, 0b101, 0b110)]
+    circ, idx = pc.bind(params)
+    z0 = np.zeros(1 << n, complex)
+    z0[0] = 1
+    ev, g = oracle.adjoint_grad(z0, n, circ, idx, pc.nparams, terms)
+    assert abs(ev - oracle.pauli_expval(oracle.apply_circuit(z0, n, circ), n, terms)) < 1e-12
+    assert np.abs(g - oracle.param_shift_grad(pc, params, terms)).max() < 1e-11
