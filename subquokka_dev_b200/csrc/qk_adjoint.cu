@@ -162,6 +162,9 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_rot(C *__restrict__ psi, C 
 int launch_gate_op(void *state, int n, int dtype, const Op &op, cudaStream_t st);
 
 static int cuda_err(cudaError_t e, const char *what) {
+    // An allocation failure is not sticky, but it stays as the thread's last
+    // error; clear it so the next launch check does not report it again.
+    if (e == cudaErrorMemoryAllocation) (void)cudaGetLastError();
     return fail(e == cudaErrorMemoryAllocation ? QK_ERR_OOM : QK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 

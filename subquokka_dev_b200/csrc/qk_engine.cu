@@ -57,6 +57,9 @@ __global__ void k_c64_to_c128(const float2 *in, double2 *out, uint64_t namp) {
 }
 
 static int cuda_fail(cudaError_t e, const char *what) {
+    // An allocation failure is not sticky, but it stays as the thread's last
+    // error; clear it so the next launch check does not report it again.
+    if (e == cudaErrorMemoryAllocation) (void)cudaGetLastError();
     return fail(e == cudaErrorMemoryAllocation ? QK_ERR_OOM : QK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 

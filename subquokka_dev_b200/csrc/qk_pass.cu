@@ -132,6 +132,9 @@ __global__ void k_perm_flat(C *__restrict__ s, uint64_t namp, PassDesc d) {
 }
 
 static int cuda_err(cudaError_t e, const char *what) {
+    // An allocation failure is not sticky, but it stays as the thread's last
+    // error; clear it so the next launch check does not report it again.
+    if (e == cudaErrorMemoryAllocation) (void)cudaGetLastError();
     return fail(e == cudaErrorMemoryAllocation ? QK_ERR_OOM : QK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
