@@ -2,22 +2,34 @@
 //
 // A block is a 64 x 64 complex unitary U on six qubits (the product of
 // consecutive gates, built on the host in FP64).  A pass applies one block to
-// the whole state.  Each CTA owns one SM, loads the block's operand A once,
-// and streams 4096-amplitude tiles (the block's six qubits plus six more
-// tile bits, the lowest state bits first for coalescing):
+// the whole state.  Each CTA owns one SM, loads the block's operand once,
+// and streams supertiles of 64 x 128 amplitudes (the block's six qubits plus
+// the lowest seven other state bits; 64 x 64 at 12 qubits):
 //
-//   tile as X[i][n]: i = block-qubit index (64), n = other tile bits (64)
-//   real embedding, rows/cols interleaved (2i + re/im):
-//     A[2i'+a][2i+b] = [[Ur, -Ui], [Ui, Ur]][a][b](i', i)      (128 x 128)
-//     D[m][n] = sum_k A[m][k] B[n][k],  B[n][2i+b] = (re, im)_b X[i][n]
+//   supertile as X[i][n]: i = block-qubit index (64), n = other tile bits (128)
+//   real embedding, columns interleaved (2i + re/im):
+//     S[n][2i+b]  = (re, im)_b X[i][n]                           (128 x 128)
+//     W[2i'+a][2i+b] = [[Ur, -Ui], [Ui, Ur]][a][b](i', i)         (128 x 128)
+//     D[n][m] = sum_k S[n][k] W[m][k]   ->  X'[i'][n] = D[n][2i'] + i D[n][2i'+1]
 //   split precision (3 x BF16, FP32 accumulate in TMEM):
-//     A = Ah + Al, B = Bh + Bl,  D = Ah Bh + Ah Bl + Al Bh   (K = 3 x 128)
+//     S = Sh + Sl, W = Wh + Wl,  D = Sh Wh + Sl Wh + Sh Wl   (K = 3 x 128)
 //
-// 24 tcgen05.mma (M128 N64 K16, kind::f16 with BF16 operands) per tile, issued
-// by one thread, completion through tcgen05.commit -> mbarrier.  Operands sit
-// in shared memory in the canonical K-major no-swizzle layout: 8-row x 16-byte
-// core matrices, LBO = 128 B between K chunks, SBO = 2048 B between row
-// groups.  The next tile is prefetched with cp.async during the contraction.
+// 24 tcgen05.mma (M128 N128 K16, kind::f16, BF16 operands) per supertile,
+// issued by one thread, completion through tcgen05.commit -> mbarrier.  The
+// state is the M operand so that TMEM lane = state row n: after tcgen05.ld a
+// thread holds whole (re, im) pairs of one row, and a warp's stores run along
+// n, the contiguous direction of the state whenever the block does not own
+// qubit 0.  Operands sit in shared memory in the canonical K-major
+// no-swizzle layout: 8-row x 16-byte core matrices, LBO = 128 B between K
+// chunks, SBO = 2048 B between row groups.
+//
+// Pipeline per CTA (state operand double-buffered in shared memory, two
+// accumulators in TMEM): convert supertile s into buffer s % 2, issue its
+// contraction, load supertile s + 2 grid into the registers it came from
+// (two register sets keep two supertiles of loads in flight), then wait for
+// contraction s - 1 and drain its accumulator straight to HBM.  Each thread
+// loads and stores the same 16 amplitudes of every supertile (row n, block
+// indices 16 (tid / 128) ..).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -30,17 +42,16 @@
 
 namespace qk {
 
-constexpr int kTcThreads = 256;
-constexpr int kTcTileBits = 12;
-constexpr uint32_t kTcTile = 1u << kTcTileBits;       // amplitudes per tile
+constexpr int kTcThreads = 512;
+constexpr int kTcMaxTileBits = 13;                    // 64 x 128 amplitudes
+constexpr int kTcMinTileBits = 12;                    // 64 x 64
 constexpr uint32_t kTcOpBytes = 128 * 128 * 2;        // one 128 x 128 bf16 operand
-constexpr uint32_t kTcBBytes = 64 * 128 * 2;          // one 64 x 128 bf16 operand
-constexpr uint32_t kTcTmemCols = 64;
-constexpr uint32_t kTcSmem = 2 * kTcTile * 8 + 2 * kTcOpBytes + 2 * kTcBBytes + 256;
+constexpr uint32_t kTcSmem = 6 * kTcOpBytes;          // W hi/lo + two state buffers hi/lo
+constexpr uint32_t kTcTmemCols = 256;                 // two 128-column accumulators
 constexpr long long kTcWaitLimit = 20000000;          // mbarrier polls before giving up
 
 struct DenseDesc {
-    PassDesc p;         // tile bits (T = 12), L
+    PassDesc p;         // tile bits (T = 13, or 12), L
     uint32_t blockmask; // tile-local bits that are the block's qubits
 };
 
@@ -51,11 +62,6 @@ __host__ __device__ __forceinline__ uint32_t kmajor_off(uint32_t r, uint32_t k) 
 
 __device__ __forceinline__ uint32_t s_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Shared-memory position of tile element j: the 16-byte pair (j, j ^ 1) stays
-// together (cp.async granule); the pair index is XORed with a fold of the
-// higher index bits so that strided block-qubit accesses spread over banks.
-__device__ __forceinline__ uint32_t tcz(uint32_t j) { return j ^ ((((j >> 4) ^ (j >> 7) ^ (j >> 10)) & 7u) << 1); }
-
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
     d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;   // leading byte offset: next K chunk
@@ -64,8 +70,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     return d;                                       // base offset 0, no swizzle
 }
 
-// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 64
-constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -81,30 +87,59 @@ __device__ __forceinline__ void store_bf16x8(unsigned char *dst, const float *v)
     *reinterpret_cast<uint4 *>(dst) = w;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__ s, uint64_t ntiles,
+// Bounded wait for the phase with parity `parity` of bar.
+__device__ __forceinline__ uint32_t tc_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done = 0;
+    for (long long t = 0; t < kTcWaitLimit && !done; ++t) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(s_u32(bar)), "r"(parity)
+            : "memory");
+    }
+    return done;
+}
+
+// Per-thread work of one supertile, two layouts:
+//
+// STATE_M (the block does not own qubit 0; the supertile's n index runs along
+// the contiguous direction of the state): the state is the M operand,
+// D[n][m] = sum_k S[n][k] W[m][k], TMEM lane = row n.  Thread t owns row
+// n = t % 128 and block indices 16 (t / 128) .. + 15: it loads them (warp
+// lanes along n), converts them into 16-byte K chunks, and drains the same
+// amplitudes from TMEM lane n, columns 32 (t / 128) .. + 31.
+//
+// STATE_N (the block owns qubit 0; block indices run along the contiguous
+// direction): the state is the N operand, D[m][n] = sum_k W[m][k] S[n][k],
+// TMEM lane = m = 2 i' + re/im.  Loads take chunks of four consecutive block
+// indices (two 16-byte vectors) with warp lanes over n bits 0-2 and chunk
+// bits 0-1; the drain pairs re/im lanes with one shuffle so that each lane
+// stores whole amplitudes, the warp's stores running along i'.
+//
+// NROWS = state rows per supertile: 128, or 64 for a 12-qubit state (rows
+// 64..127 of the state operand then stay zero and are not stored).
+template <int NROWS, bool STATE_N>
+__global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__ s, uint64_t nsup,
                                                             const __grid_constant__ DenseDesc dd,
-                                                            const uint16_t *__restrict__ gA, int *__restrict__ err) {
+                                                            const uint16_t *__restrict__ gW, int *__restrict__ err) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
     const PassDesc &d = dd.p;
-    float2 *buf0 = reinterpret_cast<float2 *>(sm);
-    float2 *buf1 = buf0 + kTcTile;
-    unsigned char *Ah = sm + 2 * kTcTile * 8;
-    unsigned char *Al = Ah + kTcOpBytes;
-    unsigned char *Bh = Al + kTcOpBytes;
-    unsigned char *Bl = Bh + kTcBBytes;
-    uint16_t *jb = reinterpret_cast<uint16_t *>(Bl + kTcBBytes);
-    uint16_t *jo = jb + 64;
+    unsigned char *Wh = sm;
+    unsigned char *Wl = Wh + kTcOpBytes;
+    unsigned char *S0 = Wl + kTcOpBytes;    // buffer b: hi at S0 + 2b op, lo after it
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // operand A (hi, lo) for the whole kernel, index tables, barrier, TMEM
     for (uint32_t i = tid; i < 2 * kTcOpBytes / 16; i += kTcThreads)
-        reinterpret_cast<uint4 *>(Ah)[i] = reinterpret_cast<const uint4 *>(gA)[i];
-    if (tid < 64) jb[tid] = (uint16_t)deposit_bits(tid, dd.blockmask);
-    else if (tid < 128) jo[tid - 64] = (uint16_t)deposit_bits(tid - 64, (kTcTile - 1) & ~dd.blockmask);
+        reinterpret_cast<uint4 *>(Wh)[i] = reinterpret_cast<const uint4 *>(gW)[i];
+    if (NROWS < 128)
+        for (uint32_t i = tid; i < 4 * kTcOpBytes / 16; i += kTcThreads)
+            reinterpret_cast<uint4 *>(S0)[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&bar)), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&bar[0])), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&bar[1])), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -113,135 +148,219 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+
+    // state offsets of the tile's index bits: jn(n) for the other index,
+    // jb(i) for the block index (both linear in the bits)
+    const uint32_t tmask = (1u << d.T) - 1, nmask = tmask & ~dd.blockmask;
+    auto jn = [&](uint32_t v) { return pass_off(deposit_bits(v, nmask), d); };
+    auto jb = [&](uint32_t v) { return pass_off(deposit_bits(v, dd.blockmask), d); };
+
+    // STATE_M: row n, offset of amplitude k = lrow + sum of le[b], b in bits(k)
+    // STATE_N: load chunk u at lrow + lu[u] (+ lpair for its second pair);
+    //          drain lane: row drow, column k at drow + sum of de[b], b in bits(k)
+    uint32_t n_m = 0, cg_m = 0;
+    bool active = true;
+    uint64_t lrow = 0, le[4] = {0, 0, 0, 0}, lu[2] = {0, 0}, lpair = 0, drow = 0, de[4] = {0, 0, 0, 0};
+    uint32_t conv_n = 0, conv_c = 0;
+    if constexpr (!STATE_N) {
+        n_m = tid & 127;
+        cg_m = tid >> 7;
+        active = n_m < NROWS;
+        lrow = jn(n_m) + jb(16 * cg_m);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) le[b] = jb(1u << b);
+    } else {
+        // chunk (n, c), n = (t & 7) | ((t >> 7) & 3) << 3 | u << 5, c = (t >> 3) & 15
+        conv_n = (tid & 7) | (((tid >> 7) & 3) << 3);
+        conv_c = (tid >> 3) & 15;
+        lrow = jn(conv_n) + jb(4 * conv_c);
+        lu[0] = jn(32);
+        lu[1] = jn(64);
+        lpair = jb(2);
+        // drain: lanes m = 32 (warp % 4) + lane, columns 32 (warp / 4) + 16 h + 2 j + (lane & 1)
+        drow = jb(16 * (warp & 3) + (lane >> 1)) + jn(32 * (warp >> 2) + (lane & 1));
+#pragma unroll
+        for (int b = 0; b < 4; ++b) de[b] = jn(2u << b);
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
+    constexpr int NU = STATE_N ? NROWS / 32 : 4;   // STATE_N: chunks per thread
 
-    // tile addressing: thread handles amplitude pairs p = tid + 256 u (u < 8),
-    // elements j = 2p, 2p + 1 (tile bit 0 is state bit 0: 16-byte runs)
-    const uint64_t g_t = pass_off(2 * tid, d);
-    uint64_t g_u[3];
+    auto load = [&](float2 (&x)[16], const float2 *p) {
+        if constexpr (!STATE_N) {
+            if (active) {
+                const float2 *q[16];
+                q[0] = p + lrow;
 #pragma unroll
-    for (int b = 0; b < 3; ++b) g_u[b] = pass_off(512u << b, d);
-    auto goff = [&](int u) {
-        uint64_t x = g_t;
+                for (int k = 1; k < 16; ++k) q[k] = q[k & (k - 1)] + le[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
 #pragma unroll
-        for (int b = 0; b < 3; ++b)
-            if ((u >> b) & 1) x |= g_u[b];
-        return x;
-    };
-    auto prefetch = [&](float2 *buf, uint64_t base) {
+                for (int k = 0; k < 16; ++k) x[k] = *q[k];
+            }
+        } else {
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const uint32_t j = 2 * (tid + 256 * u);
-            const uint32_t dst = s_u32(buf + tcz(j));
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(s + (base | goff(u))) : "memory");
-        }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
-
-    uint32_t phase = 0;
-    uint64_t o = blockIdx.x;
-    if (o < ntiles) prefetch(buf0, pass_base(o, d));
-    for (int it = 0; o < ntiles; o += gridDim.x, ++it) {
-        float2 *tl = (it & 1) ? buf1 : buf0;
-        float2 *nx = (it & 1) ? buf0 : buf1;
-        const uint64_t base = pass_base(o, d);
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();
-        if (o + gridDim.x < ntiles) prefetch(nx, pass_base(o + gridDim.x, d));
-
-        // B operand: row n = tid / 4, K columns 2i + b for i in [16 (tid % 4), +16)
-        {
-            const uint32_t n = tid >> 2, i0 = (tid & 3) * 16;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                float hi[8], lo[8];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float2 x = tl[tcz(jb[i0 + 4 * c + q] | jo[n])];
-                    const float xs[2] = {x.x, x.y};
-#pragma unroll
-                    for (int b = 0; b < 2; ++b) {
-                        const float h = __bfloat162float(__float2bfloat16_rn(xs[b]));
-                        hi[2 * q + b] = h;
-                        lo[2 * q + b] = xs[b] - h;
-                    }
-                }
-                const uint32_t off = kmajor_off(n, 2 * i0 + 8 * c);
-                store_bf16x8(Bh + off, hi);
-                store_bf16x8(Bl + off, lo);
+            for (int u = 0; u < NU; ++u) {
+                const float2 *q = p + lrow + (u & 1 ? lu[0] : 0) + (u & 2 ? lu[1] : 0);
+                const float4 v0 = *reinterpret_cast<const float4 *>(q);
+                const float4 v1 = *reinterpret_cast<const float4 *>(q + lpair);
+                x[4 * u + 0] = make_float2(v0.x, v0.y);
+                x[4 * u + 1] = make_float2(v0.z, v0.w);
+                x[4 * u + 2] = make_float2(v1.x, v1.y);
+                x[4 * u + 3] = make_float2(v1.z, v1.w);
             }
         }
+    };
+    // four amplitudes (consecutive block indices) -> one 16-byte hi and lo chunk
+    auto chunk = [&](const float2 *x4, unsigned char *Sh, unsigned char *Sl, uint32_t o) {
+        float hi[8], lo[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float xs[2] = {x4[q].x, x4[q].y};
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const float h = __bfloat162float(__float2bfloat16_rn(xs[b]));
+                hi[2 * q + b] = h;
+                lo[2 * q + b] = xs[b] - h;
+            }
+        }
+        store_bf16x8(Sh + o, hi);
+        store_bf16x8(Sl + o, lo);
+    };
+    auto convert = [&](const float2 (&x)[16], unsigned char *Sh, unsigned char *Sl) {
+        if constexpr (!STATE_N) {
+            if (!active) return;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) chunk(x + 4 * c, Sh, Sl, kmajor_off(n_m, 2 * (16 * cg_m + 4 * c)));
+        } else {
+#pragma unroll
+            for (int u = 0; u < NU; ++u) chunk(x + 4 * u, Sh, Sl, kmajor_off(conv_n | (u << 5), 8 * conv_c));
+        }
+    };
+    auto issue = [&](const unsigned char *Sh, const unsigned char *Sl, uint32_t acc_col, uint64_t *b) {
+#pragma unroll 1
+        for (int sp = 0; sp < 3; ++sp) {   // S W products: hi hi, lo hi, hi lo
+            const uint32_t sa = s_u32(sp == 1 ? Sl : Sh), w = s_u32(sp == 2 ? Wl : Wh);
+#pragma unroll 1
+            for (int kk = 0; kk < 8; ++kk) {
+                const uint64_t sd = umma_desc(sa + kk * 256), wd = umma_desc(w + kk * 256);
+                const uint64_t ad = STATE_N ? wd : sd, bd = STATE_N ? sd : wd;
+                const uint32_t acc = (sp | kk) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                        tmem + acc_col),
+                    "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_u32(b))
+                     : "memory");
+    };
+    auto tmem_ld16 = [&](uint32_t taddr, uint32_t (&r)[16]) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+            "%13, %14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    };
+    auto drain = [&](uint32_t acc_col, float2 *p) {
+        const uint32_t lane_base = tmem + ((32u * (uint32_t)(warp & 3)) << 16) + acc_col + 32u * (uint32_t)(warp >> 2);
+        if constexpr (!STATE_N) {
+            // two 16-column halves (8 amplitudes each) of row n
+            float2 *q[16];
+            q[0] = p + lrow;
+#pragma unroll
+            for (int k = 1; k < 16; ++k) q[k] = q[k & (k - 1)] + le[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t r[16];
+                tmem_ld16(lane_base + 16u * h, r);
+                if (active) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        *q[8 * h + k] = make_float2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1]));
+                }
+            }
+        } else {
+            // lane holds one of re/im of block index i' for 32 columns n;
+            // after the swap, lane (re) stores even n, lane (im) odd n
+            const uint32_t comp = lane & 1;
+            float2 *q[16];
+            q[0] = p + drow;
+#pragma unroll
+            for (int k = 1; k < 16; ++k) q[k] = q[k & (k - 1)] + de[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t r[16];
+                tmem_ld16(lane_base + 16u * h, r);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float keep = __uint_as_float(comp ? r[2 * j + 1] : r[2 * j]);
+                    const float send = __uint_as_float(comp ? r[2 * j] : r[2 * j + 1]);
+                    const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+                    if (32 * (warp >> 2) + 16 * h + 2 * j < NROWS)
+                        *q[8 * h + j] = comp ? make_float2(recv, keep) : make_float2(keep, recv);
+                }
+            }
+        }
+    };
+
+    // one supertile: convert x (supertile o) into buffer it % 2, start its
+    // contraction, refill x with supertile o + 2 grid, drain supertile it - 1
+    uint32_t it = 0;
+    bool bad = false;
+    float2 *prev = s;
+    auto step = [&](float2 (&x)[16], uint64_t o) {
+        const uint32_t b = it & 1;
+        unsigned char *Sh = S0 + 2 * b * kTcOpBytes, *Sl = Sh + kTcOpBytes;
+        convert(x, Sh, Sl);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
-        if (tid == 0) {
-#pragma unroll 1
-            for (int sp = 0; sp < 3; ++sp) {
-                const uint32_t a = s_u32(sp < 2 ? Ah : Al), b = s_u32(sp == 1 ? Bl : Bh);
-#pragma unroll 1
-                for (int kk = 0; kk < 8; ++kk) {
-                    const uint64_t ad = umma_desc(a + kk * 256), bd = umma_desc(b + kk * 256);
-                    const uint32_t acc = (sp | kk) ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                        "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-                        : "memory");
-                }
+        if (tid == 0) issue(Sh, Sl, b * 128u, &bar[b]);
+        __syncwarp();   // warp 0 reconverges before its aligned tcgen05 ops
+        if (o + 2ull * gridDim.x < nsup) load(x, s + pass_base(o + 2ull * gridDim.x, d));
+        if (it > 0) {
+            const uint32_t pb = b ^ 1u;
+            if (__syncthreads_or(!tc_wait(&bar[pb], ((it - 1) >> 1) & 1u))) {
+                bad = true;
+                return;
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_u32(&bar))
-                         : "memory");
+            tc_fence_after();
+            drain(pb * 128u, prev);
+            tc_fence_before();
         }
-        // bounded wait for the contraction
-        uint32_t done = 0;
-        for (long long t = 0; t < kTcWaitLimit && !done; ++t) {
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                "selp.u32 %0, 1, 0, p;\n\t}\n"
-                : "=r"(done)
-                : "r"(s_u32(&bar)), "r"(phase)
-                : "memory");
-        }
-        phase ^= 1u;
-        if (__syncthreads_or(!done)) {
-            if (tid == 0) atomicExch(err, 1);
-            break;
-        }
-        tc_fence_after();
-        // D rows m = 32 (warp % 4) + lane, columns 32 (warp / 4) .. + 32
-        {
-            uint32_t r[32];
-            const uint32_t taddr = tmem + (((uint32_t)(warp & 3) * 32u) << 16) + 32u * (uint32_t)(warp >> 2);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-                  "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
-                  "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-                  "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const uint32_t m = (uint32_t)(warp & 3) * 32u + lane, ip = m >> 1, comp = m & 1;
-            const uint32_t n0 = 32u * (uint32_t)(warp >> 2);
-#pragma unroll
-            for (int q = 0; q < 32; ++q)
-                reinterpret_cast<float *>(&tl[tcz(jb[ip] | jo[n0 + q])])[comp] = __uint_as_float(r[q]);
-        }
-        tc_fence_before();
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const uint32_t j = 2 * (tid + 256 * u);
-            *reinterpret_cast<float4 *>(s + (base | goff(u))) = *reinterpret_cast<const float4 *>(tl + tcz(j));
+        prev = s + pass_base(o, d);
+        ++it;
+    };
+
+    float2 xa[16], xb[16];
+    uint64_t o = blockIdx.x;
+    if (o < nsup) load(xa, s + pass_base(o, d));
+    if (o + gridDim.x < nsup) load(xb, s + pass_base(o + gridDim.x, d));
+    while (o < nsup) {
+        step(xa, o);
+        o += gridDim.x;
+        if (bad || o >= nsup) break;
+        step(xb, o);
+        o += gridDim.x;
+        if (bad) break;
+    }
+    if (!bad && it > 0) {
+        const uint32_t pb = (it - 1) & 1u;
+        if (__syncthreads_or(!tc_wait(&bar[pb], ((it - 1) >> 1) & 1u))) {
+            bad = true;
+        } else {
+            tc_fence_after();
+            drain(pb * 128u, prev);
         }
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (bad && tid == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -264,7 +383,7 @@ static float bf16_to_f(uint16_t h) {
     return f;
 }
 
-// A = real embedding of U (rows/cols interleaved re/im), split into bf16 hi +
+// W = real embedding of U (rows/cols interleaved re/im), split into bf16 hi +
 // lo, each in the canonical K-major layout: 2 x 32 KiB.
 void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out) {
     out.assign(2 * 128 * 128, 0);
@@ -286,14 +405,16 @@ void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out) {
         }
 }
 
-// tile bits of a block: its six qubits plus the lowest other state bits
+// tile bits of a block: its six qubits plus the lowest other state bits, up
+// to 13 (64 x 128 supertiles)
 DenseDesc dense_block_desc(const DenseBlock &b, int n) {
     DenseDesc dd;
     std::memset(&dd, 0, sizeof dd);
     std::vector<char> in(n, 0);
     for (int k = 0; k < kDenseQubits; ++k) in[b.q[k]] = 1;
+    const int tbits = std::min(n, kTcMaxTileBits);
     int cnt = kDenseQubits;
-    for (int q = 0; q < n && cnt < kTcTileBits; ++q)
+    for (int q = 0; q < n && cnt < tbits; ++q)
         if (!in[q]) { in[q] = 1; ++cnt; }
     int t = 0;
     for (int q = 0; q < n; ++q)
@@ -307,22 +428,35 @@ DenseDesc dense_block_desc(const DenseBlock &b, int n) {
     return dd;
 }
 
-int launch_dense_tc(float2 *state, int n, const DenseDesc &dd, const uint16_t *dA, int *derr, cudaStream_t st) {
+template <int NROWS, bool STATE_N>
+static int launch_dense_tc_n(float2 *state, int n, const DenseDesc &dd, const uint16_t *dW, int *derr,
+                             cudaStream_t st) {
     static int sms = 0;
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e = cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+        cudaError_t e =
+            cudaFuncSetAttribute(k_dense_tc<NROWS, STATE_N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
         if (e != cudaSuccess) return fail(QK_ERR_CUDA, "cudaFuncSetAttribute(k_dense_tc): %s", cudaGetErrorString(e));
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    if (n < kTcTileBits || dd.p.T != kTcTileBits || dd.p.L < 1)
-        return fail(QK_ERR_ARG, "tensor-core blocks need >= %d qubits", kTcTileBits);
-    const uint64_t ntiles = 1ull << (n - kTcTileBits);
-    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sms);
-    k_dense_tc<<<grid, kTcThreads, kTcSmem, st>>>(state, ntiles, dd, dA, derr);
+    const uint64_t nsup = 1ull << (n - dd.p.T);
+    const unsigned grid = (unsigned)std::min<uint64_t>(nsup, (uint64_t)sms);
+    k_dense_tc<NROWS, STATE_N><<<grid, kTcThreads, kTcSmem, st>>>(state, nsup, dd, dW, derr);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : fail(QK_ERR_CUDA, "k_dense_tc launch: %s", cudaGetErrorString(e));
+}
+
+int launch_dense_tc(float2 *state, int n, const DenseDesc &dd, const uint16_t *dW, int *derr, cudaStream_t st) {
+    if (n < kTcMinTileBits || dd.p.T < kTcMinTileBits || dd.p.T > kTcMaxTileBits || dd.p.T > n || dd.p.L < 1)
+        return fail(QK_ERR_ARG, "tensor-core blocks need >= %d qubits", kTcMinTileBits);
+    // a block on qubit 0 has its block index along the contiguous direction
+    const bool state_n = (dd.blockmask & 1u) != 0;
+    if (dd.p.T == 12)
+        return state_n ? launch_dense_tc_n<64, true>(state, n, dd, dW, derr, st)
+                       : launch_dense_tc_n<64, false>(state, n, dd, dW, derr, st);
+    return state_n ? launch_dense_tc_n<128, true>(state, n, dd, dW, derr, st)
+                   : launch_dense_tc_n<128, false>(state, n, dd, dW, derr, st);
 }
 
 // from qk_pass.cu: one VSWAP as a permutation pass

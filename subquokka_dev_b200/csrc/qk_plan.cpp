@@ -525,7 +525,9 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, std::vector<Dense
                 rest.push_back(i);
             }
         }
-        for (int q = 0; q < n && (int)Q.size() < kDenseQubits; ++q)
+        // pad with the highest free qubits (identity on them): keeping the low
+        // qubits out of a block keeps its tiles' other index contiguous
+        for (int q = n - 1; q >= 0 && (int)Q.size() < kDenseQubits; --q)
             if (std::find(Q.begin(), Q.end(), q) == Q.end()) Q.push_back(q);
         std::sort(Q.begin(), Q.end());
         DenseBlock b;
