@@ -326,7 +326,7 @@ def extra_workloads(args):
         def run():
             sv.reset()
             box["r"] = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
-        ms = time_device(run, 1, 2)
+        ms = time_device(run, 2, 3)
         ev, g, drift = box["r"]
         grads[(dtype, fused)] = g
         key = f"{dtype}_{'fused' if fused else 'per_gate'}"

@@ -163,6 +163,11 @@ int qk_sv_info(const qk_sv *sv, int *nqubits, int *dtype, void **device_ptr, siz
 int qk_sv_set_stream(qk_sv *sv, void *cuda_stream);
 /* Wait for all work queued on the state's stream. */
 int qk_sv_synchronize(qk_sv *sv);
+/* Free the device workspace that adjoint sweeps and expectation values keep
+ * with the state (lambda, checkpoints, accumulators, pass programs).  The
+ * reference has no counterpart (its runner allocates nothing besides the
+ * state, src/MEM_Runner.cpp:57-88). */
+int qk_sv_release_workspace(qk_sv *sv);
 
 /* ---- the hot path ------------------------------------------------------ */
 
@@ -258,7 +263,8 @@ int qk_expval_pauli(qk_sv *sv, const qk_pauli_term *terms, size_t nterms, double
  * receives the root sum of squared differences found there.  *expval
  * receives <H>.  On return sv holds the initial state again (uncomputed, or
  * restored from the first checkpoint).  Device memory: one extra state plus
- * the checkpoints, allocated for the call. */
+ * the checkpoints, kept by sv as its workspace for the next call (grown when
+ * a call needs more) until qk_sv_release_workspace or qk_sv_destroy. */
 int qk_adjoint_grad(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_t *param_index, size_t nparams,
                     const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
                     double *drift);

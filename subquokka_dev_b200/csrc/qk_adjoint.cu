@@ -237,7 +237,7 @@ static int generator(const qk_gate &g) {
 template <typename C>
 static int adjoint_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, const int32_t *pidx, size_t nparams,
                      const std::vector<PauliGroup> &groups, int ncheck, double *expval, double *grad, double *drift,
-                     cudaStream_t st) {
+                     Workspace &ws, cudaStream_t st) {
     const uint64_t namp = 1ull << n;
     const size_t bytes = sizeof(C) * namp;
     std::vector<Op> ops(ng);
@@ -261,40 +261,30 @@ static int adjoint_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, 
             if (c > 0 && c < ng && (cpos.empty() || c > cpos.back())) cpos.push_back(c);
         }
     }
-    C *lam = nullptr, *ck = nullptr;
-    double *dacc = nullptr;
-    cudaError_t e = cudaMalloc(&lam, bytes);
-    if (e != cudaSuccess) return cuda_err(e, "cudaMalloc(lambda)");
+    cudaError_t e = ws.reserve(bytes * (1 + cpos.size()), (nparams + 2) * sizeof(double), 0);
+    if (e != cudaSuccess) return cuda_err(e, "cudaMalloc(adjoint workspace: lambda, checkpoints)");
+    C *lam = static_cast<C *>(ws.states);
+    C *ck = lam + namp;
+    double *dacc = ws.acc;
     int rc = QK_OK;
-    auto done = [&](int code) {
-        if (lam) cudaFree(lam);
-        if (ck) cudaFree(ck);
-        if (dacc) cudaFree(dacc);
-        return code;
-    };
-    if (!cpos.empty()) {
-        e = cudaMalloc(&ck, bytes * cpos.size());
-        if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(checkpoints)"));
-    }
     const size_t nacc = nparams + 2;  // grads, expval, drift
-    e = cudaMalloc(&dacc, nacc * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
-    if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(accumulators)"));
+    e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
+    if (e != cudaSuccess) return cuda_err(e, "clear accumulators");
 
     // forward, saving checkpoints
     size_t nc = 0;
     for (size_t i = 0; i < ng; ++i) {
         if (nc < cpos.size() && cpos[nc] == i) {
             e = cudaMemcpyAsync(ck + nc * namp, psi, bytes, cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return done(cuda_err(e, "checkpoint"));
+            if (e != cudaSuccess) return cuda_err(e, "checkpoint");
             ++nc;
         }
         rc = launch_gate_op(psi, n, dtype, ops[i], st);
-        if (rc) return done(rc);
+        if (rc) return rc;
     }
     // lambda = H psi, <H> = Re<psi|lambda>
     rc = apply_h_t<C>(lam, psi, n, groups, st);
-    if (rc) return done(rc);
+    if (rc) return rc;
     k_dot_re<C><<<red_grid(namp), kRedThreads, 0, st>>>(psi, lam, namp, dacc + nparams);
     // backward
     for (size_t i = ng; i-- > 0;) {
@@ -315,28 +305,28 @@ static int adjoint_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, 
             const uint64_t np = namp / 2;
             k_adj_rot<C><<<red_grid(np), kRedThreads, 0, st>>>(psi, lam, np, inv.q[0], u, generator(gates[i]), dacc + p);
             e = cudaGetLastError();
-            if (e != cudaSuccess) return done(cuda_err(e, "k_adj_rot"));
+            if (e != cudaSuccess) return cuda_err(e, "k_adj_rot");
         } else {
             rc = launch_gate_op(psi, n, dtype, inv, st);
             if (!rc) rc = launch_gate_op(lam, n, dtype, inv, st);
-            if (rc) return done(rc);
+            if (rc) return rc;
         }
         // psi now holds the state before gate i: compare with and restore from a checkpoint
         if (nc > 0 && cpos[nc - 1] == i) {
             --nc;
             k_dist2<C><<<red_grid(namp), kRedThreads, 0, st>>>(psi, ck + nc * namp, namp, dacc + nparams + 1);
             e = cudaMemcpyAsync(psi, ck + nc * namp, bytes, cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return done(cuda_err(e, "restore checkpoint"));
+            if (e != cudaSuccess) return cuda_err(e, "restore checkpoint");
         }
     }
     std::vector<double> h(nacc);
     e = cudaMemcpyAsync(h.data(), dacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return done(cuda_err(e, "read results"));
+    if (e != cudaSuccess) return cuda_err(e, "read results");
     if (grad) std::memcpy(grad, h.data(), nparams * sizeof(double));
     if (expval) *expval = h[nparams];
     if (drift) *drift = std::sqrt(h[nparams + 1]);
-    return done(QK_OK);
+    return QK_OK;
 }
 
 // fused passes (qk_pass.cu)
@@ -353,7 +343,7 @@ int run_adjoint_plan(void *psi, void *lam, int dtype, const HostPlan &hp, const 
 template <typename C>
 static int adjoint_fused_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, const int32_t *pidx,
                            size_t nparams, const std::vector<PauliGroup> &groups, int ncheck, double *expval,
-                           double *grad, double *drift, cudaStream_t st) {
+                           double *grad, double *drift, Workspace &ws, cudaStream_t st) {
     const uint64_t namp = 1ull << n;
     const size_t bytes = sizeof(C) * namp;
     std::vector<size_t> cut{0};
@@ -374,62 +364,49 @@ static int adjoint_fused_t(C *psi, int n, int dtype, const qk_gate *gates, size_
         for (int32_t p : bwd[sgi].grad_params)
             if (p < 0 || (size_t)p >= nparams) return fail(QK_ERR_ARG, "parameter %d >= %zu", p, nparams);
     }
-    std::vector<DevPlan> dfw(nseg), dbw(nseg);
-    C *lam = nullptr, *ck = nullptr;
-    double *dacc = nullptr;
-    auto done = [&](int code) {
-        for (auto &d : dfw) d.release();
-        for (auto &d : dbw) d.release();
-        if (lam) cudaFree(lam);
-        if (ck) cudaFree(ck);
-        if (dacc) cudaFree(dacc);
-        return code;
-    };
-    for (size_t sgi = 0; sgi < nseg; ++sgi) {
-        int rc = upload_host_plan(fwd[sgi], dfw[sgi], st);
-        if (!rc) rc = upload_host_plan(bwd[sgi], dbw[sgi], st);
-        if (rc) return done(rc);
-    }
-    cudaError_t e = cudaMalloc(&lam, bytes);
-    if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(lambda)"));
-    if (nseg > 1) {
-        e = cudaMalloc(&ck, bytes * (nseg - 1));
-        if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(checkpoints)"));
-    }
     const size_t nacc = nparams + 2;
-    e = cudaMalloc(&dacc, nacc * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
-    if (e != cudaSuccess) return done(cuda_err(e, "cudaMalloc(accumulators)"));
+    cudaError_t e = ws.reserve(bytes * nseg, nacc * sizeof(double), 2 * nseg);
+    if (e != cudaSuccess) return cuda_err(e, "cudaMalloc(adjoint workspace: lambda, checkpoints)");
+    C *lam = static_cast<C *>(ws.states);
+    C *ck = lam + namp;
+    double *dacc = ws.acc;
+    for (size_t sgi = 0; sgi < nseg; ++sgi) {
+        int rc = upload_host_plan(fwd[sgi], ws.plans[2 * sgi], st);
+        if (!rc) rc = upload_host_plan(bwd[sgi], ws.plans[2 * sgi + 1], st);
+        if (rc) return rc;
+    }
+    e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
+    if (e != cudaSuccess) return cuda_err(e, "clear accumulators");
     // forward
     for (size_t sgi = 0; sgi < nseg; ++sgi) {
         if (sgi > 0) {
             e = cudaMemcpyAsync(ck + (sgi - 1) * namp, psi, bytes, cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return done(cuda_err(e, "checkpoint"));
+            if (e != cudaSuccess) return cuda_err(e, "checkpoint");
         }
-        int rc = run_forward_plan(psi, fwd[sgi], dfw[sgi], st);
-        if (rc) return done(rc);
+        int rc = run_forward_plan(psi, fwd[sgi], ws.plans[2 * sgi], st);
+        if (rc) return rc;
     }
     int rc = apply_h_t<C>(lam, psi, n, groups, st);
-    if (rc) return done(rc);
+    if (rc) return rc;
     k_dot_re<C><<<red_grid(namp), kRedThreads, 0, st>>>(psi, lam, namp, dacc + nparams);
     // backward
     for (size_t sgi = nseg; sgi-- > 0;) {
-        rc = run_adjoint_plan(psi, lam, dtype, bwd[sgi], dbw[sgi], dacc, st);
-        if (rc) return done(rc);
+        rc = run_adjoint_plan(psi, lam, dtype, bwd[sgi], ws.plans[2 * sgi + 1], dacc, st);
+        if (rc) return rc;
         if (sgi > 0) {
             k_dist2<C><<<red_grid(namp), kRedThreads, 0, st>>>(psi, ck + (sgi - 1) * namp, namp, dacc + nparams + 1);
             e = cudaMemcpyAsync(psi, ck + (sgi - 1) * namp, bytes, cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return done(cuda_err(e, "restore checkpoint"));
+            if (e != cudaSuccess) return cuda_err(e, "restore checkpoint");
         }
     }
     std::vector<double> h(nacc);
     e = cudaMemcpyAsync(h.data(), dacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return done(cuda_err(e, "read results"));
+    if (e != cudaSuccess) return cuda_err(e, "read results");
     if (grad) std::memcpy(grad, h.data(), nparams * sizeof(double));
     if (expval) *expval = h[nparams];
     if (drift) *drift = std::sqrt(h[nparams + 1]);
-    return done(QK_OK);
+    return QK_OK;
 }
 
 }  // namespace qk
@@ -442,6 +419,7 @@ cudaStream_t state_stream(const qk_sv *sv);
 void *state_ptr(const qk_sv *sv);
 int state_qubits(const qk_sv *sv);
 int state_dtype(const qk_sv *sv);
+Workspace &state_workspace(qk_sv *sv);
 }  // namespace qk
 
 extern "C" {
@@ -453,13 +431,12 @@ int qk_expval_pauli(qk_sv *sv, const qk_pauli_term *terms, size_t nterms, double
     int rc = group_terms(terms, nterms, n, groups);
     if (rc) return rc;
     cudaStream_t st = state_stream(sv);
-    double *dacc = nullptr;
-    cudaError_t e = cudaMalloc(&dacc, sizeof(double));
-    if (e == cudaSuccess) e = cudaMemsetAsync(dacc, 0, sizeof(double), st);
-    if (e != cudaSuccess) {
-        if (dacc) cudaFree(dacc);
-        return cuda_err(e, "cudaMalloc(accumulator)");
-    }
+    Workspace &ws = state_workspace(sv);
+    cudaError_t e = ws.reserve(0, sizeof(double), 0);
+    if (e != cudaSuccess) return cuda_err(e, "cudaMalloc(accumulator)");
+    double *dacc = ws.acc;
+    e = cudaMemsetAsync(dacc, 0, sizeof(double), st);
+    if (e != cudaSuccess) return cuda_err(e, "clear accumulator");
     rc = state_dtype(sv) == QK_C128 ? expval_t<double2>((const double2 *)state_ptr(sv), n, groups, dacc, st)
                                     : expval_t<float2>((const float2 *)state_ptr(sv), n, groups, dacc, st);
     if (!rc) {
@@ -467,7 +444,6 @@ int qk_expval_pauli(qk_sv *sv, const qk_pauli_term *terms, size_t nterms, double
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = cuda_err(e, "read expectation");
     }
-    cudaFree(dacc);
     return rc;
 }
 
@@ -485,9 +461,9 @@ int qk_adjoint_grad(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_
     cudaStream_t st = state_stream(sv);
     if (dtype == QK_C128)
         return adjoint_t<double2>((double2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams, groups,
-                                  checkpoints, expval, grad, drift, st);
+                                  checkpoints, expval, grad, drift, state_workspace(sv), st);
     return adjoint_t<float2>((float2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams, groups,
-                             checkpoints, expval, grad, drift, st);
+                             checkpoints, expval, grad, drift, state_workspace(sv), st);
 }
 
 int qk_adjoint_grad_fused(qk_sv *sv, const qk_gate *gates, size_t ngates, const int32_t *param_index, size_t nparams,
@@ -504,9 +480,9 @@ int qk_adjoint_grad_fused(qk_sv *sv, const qk_gate *gates, size_t ngates, const 
     cudaStream_t st = state_stream(sv);
     if (dtype == QK_C128)
         return adjoint_fused_t<double2>((double2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams,
-                                        groups, checkpoints, expval, grad, drift, st);
+                                        groups, checkpoints, expval, grad, drift, state_workspace(sv), st);
     return adjoint_fused_t<float2>((float2 *)state_ptr(sv), n, dtype, gates, ngates, param_index, nparams, groups,
-                                   checkpoints, expval, grad, drift, st);
+                                   checkpoints, expval, grad, drift, state_workspace(sv), st);
 }
 
 }  // extern "C"

@@ -309,6 +309,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
         }
     };
 
+    // Each warp waits for a contraction on its own (lane 0 polls, bounded);
+    // a timeout is recorded in bad_s and seen by every thread after the next
+    // CTA barrier, so all threads leave the loop together.
+    __shared__ int bad_s;
+    if (tid == 0) bad_s = 0;
+    auto wait_warp = [&](uint64_t *bb, uint32_t parity) -> uint32_t {
+        uint32_t dn = 0;
+        if (lane == 0) dn = tc_wait(bb, parity);
+        return __shfl_sync(0xffffffffu, dn, 0);
+    };
+
     // one supertile: convert x (supertile o) into buffer it % 2, start its
     // contraction, refill x with supertile o + 2 grid, drain supertile it - 1
     uint32_t it = 0;
@@ -317,22 +328,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
     auto step = [&](float2 (&x)[16], uint64_t o) {
         const uint32_t b = it & 1;
         unsigned char *Sh = S0 + 2 * b * kTcOpBytes, *Sl = Sh + kTcOpBytes;
+        // buffer b and accumulator b were released by this warp's wait and
+        // drain of supertile it - 2 (and every warp's, by the barrier below)
         convert(x, Sh, Sl);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
+        if (bad_s) {
+            bad = true;
+            return;
+        }
         if (tid == 0) issue(Sh, Sl, b * 128u, &bar[b]);
         __syncwarp();   // warp 0 reconverges before its aligned tcgen05 ops
         if (o + 2ull * gridDim.x < nsup) load(x, s + pass_base(o + 2ull * gridDim.x, d));
         if (it > 0) {
             const uint32_t pb = b ^ 1u;
-            if (__syncthreads_or(!tc_wait(&bar[pb], ((it - 1) >> 1) & 1u))) {
-                bad = true;
-                return;
+            if (wait_warp(&bar[pb], ((it - 1) >> 1) & 1u)) {
+                tc_fence_after();
+                drain(pb * 128u, prev);
+            } else if (lane == 0) {
+                bad_s = 1;
             }
-            tc_fence_after();
-            drain(pb * 128u, prev);
             tc_fence_before();
         }
         prev = s + pass_base(o, d);
@@ -353,14 +370,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
     }
     if (!bad && it > 0) {
         const uint32_t pb = (it - 1) & 1u;
-        if (__syncthreads_or(!tc_wait(&bar[pb], ((it - 1) >> 1) & 1u))) {
-            bad = true;
-        } else {
+        if (wait_warp(&bar[pb], ((it - 1) >> 1) & 1u)) {
             tc_fence_after();
             drain(pb * 128u, prev);
+        } else if (lane == 0) {
+            bad_s = 1;
         }
     }
-    if (bad && tid == 0) atomicExch(err, 1);
+    __syncthreads();
+    if (bad_s && tid == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();

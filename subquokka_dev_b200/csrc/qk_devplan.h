@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cstddef>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "qk_internal.h"
@@ -22,6 +24,49 @@ struct DevPlan {
         coef = nullptr;
         gparams = nullptr;
         ops_cap = coef_cap = gparams_cap = 0;
+    }
+};
+
+// Device memory a state handle keeps between adjoint calls: the lambda state
+// and checkpoints, the accumulators and the pass programs.  Grow-only; freed
+// with the state or by qk_sv_release_workspace.
+struct Workspace {
+    void *states = nullptr;      // lambda + checkpoints
+    size_t states_cap = 0;       // bytes
+    double *acc = nullptr;       // gradient / <H> / drift accumulators
+    size_t acc_cap = 0;          // bytes
+    std::vector<DevPlan> plans;  // device programs of the sweep's passes
+
+    // Make room for `states_bytes` of states, `acc_bytes` of accumulators and
+    // `nplans` device plans.  Returns a cudaError_t.
+    cudaError_t reserve(size_t states_bytes, size_t acc_bytes, size_t nplans) {
+        if (states_bytes > states_cap) {
+            if (states) cudaFree(states);
+            states = nullptr;
+            states_cap = 0;
+            cudaError_t e = cudaMalloc(&states, states_bytes);
+            if (e != cudaSuccess) return e;
+            states_cap = states_bytes;
+        }
+        if (acc_bytes > acc_cap) {
+            if (acc) cudaFree(acc);
+            acc = nullptr;
+            acc_cap = 0;
+            cudaError_t e = cudaMalloc(&acc, acc_bytes);
+            if (e != cudaSuccess) return e;
+            acc_cap = acc_bytes;
+        }
+        if (plans.size() < nplans) plans.resize(nplans);
+        return cudaSuccess;
+    }
+    void release() {
+        if (states) cudaFree(states);
+        if (acc) cudaFree(acc);
+        states = nullptr;
+        acc = nullptr;
+        states_cap = acc_cap = 0;
+        for (auto &p : plans) p.release();
+        plans.clear();
     }
 };
 

@@ -35,6 +35,7 @@ struct qk_sv {
     size_t bytes = 0;
     cudaStream_t stream = nullptr;
     qk::DevPlan scratch;
+    qk::Workspace ws;   // adjoint sweeps: lambda, checkpoints, programs
     int device = 0;
 };
 
@@ -43,6 +44,7 @@ namespace qk {
 DevPlan &state_scratch_plan(qk_sv *sv) { return sv->scratch; }
 cudaStream_t state_stream(const qk_sv *sv) { return sv->stream; }
 void *state_ptr(const qk_sv *sv) { return sv->d; }
+Workspace &state_workspace(qk_sv *sv) { return sv->ws; }
 int state_qubits(const qk_sv *sv) { return sv->n; }
 int state_dtype(const qk_sv *sv) { return sv->dtype; }
 
@@ -192,7 +194,15 @@ void qk_sv_destroy(qk_sv *sv) {
     if (!sv) return;
     if (sv->d) cudaFree(sv->d);
     release_scratch_plan(sv->scratch);
+    sv->ws.release();
     delete sv;
+}
+
+int qk_sv_release_workspace(qk_sv *sv) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    sv->ws.release();
+    clear_error();
+    return QK_OK;
 }
 
 int qk_sv_reset(qk_sv *sv) {

@@ -225,6 +225,10 @@ class StateVector:
     def synchronize(self) -> None:
         check(self._lib.qk_sv_synchronize(self.h))
 
+    def release_workspace(self) -> None:
+        """Free the device memory adjoint sweeps keep with this state."""
+        check(self._lib.qk_sv_release_workspace(self.h))
+
     def apply(self, circuit: Circuit) -> None:
         """Per-gate path (MEM_Runner::run(vector<Gate*>&))."""
         check(self._lib.qk_apply_gates(self.h, circuit.gates, circuit.ngates))

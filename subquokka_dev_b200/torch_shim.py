@@ -40,6 +40,20 @@ class ParamCircuit:
         self.rot("RY", q, p_theta)
         self.rot("RZ", q, p_phi)
 
+    def state(self, dtype: str) -> StateVector:
+        """This circuit's device state in `dtype`, reset to |0...0>: kept between
+        calls together with its adjoint workspace; `close` frees them."""
+        states = self.__dict__.setdefault("_states", {})
+        sv = states.get(dtype)
+        if sv is None:
+            sv = states[dtype] = StateVector(self.n, dtype)
+        sv.reset()
+        return sv
+
+    def close(self) -> None:
+        for sv in self.__dict__.pop("_states", {}).values():
+            sv.close()
+
     def bind(self, params: np.ndarray):
         """(Circuit with the parameter values in place, param_index array)."""
         gates, idx = [], []
@@ -55,8 +69,8 @@ class _Expectation(torch.autograd.Function):
     def forward(ctx, params, pc, terms, dtype, checkpoints, fused):
         p = params.detach().to("cpu", torch.float64).numpy()
         circ, idx = pc.bind(p)
-        with StateVector(pc.n, dtype) as sv:
-            ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, checkpoints, fused)
+        sv = pc.state(dtype)
+        ev, grad, drift = adjoint_grad(sv, circ, idx, pc.nparams, terms, checkpoints, fused)
         ctx.save_for_backward(torch.as_tensor(grad, dtype=params.dtype, device=params.device))
         ctx.drift = drift
         return torch.tensor(ev, dtype=params.dtype, device=params.device)

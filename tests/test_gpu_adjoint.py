@@ -143,3 +143,27 @@ def test_adjoint_matches_c_restatement(fused):
         ev, g, _ = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
     assert abs(ev - ev0) < 1e-12
     assert np.abs(g - g0).max() < 1e-11
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_workspace_reuse_and_release(fused):
+    # the lambda / checkpoint workspace stays with the state between calls,
+    # grows when a call needs more checkpoints, and can be released; results
+    # do not depend on its history
+    n, layers = 11, 4
+    pc, params, terms = hea_problem(n, layers, 28)
+    circ, idx = pc.bind(params)
+    with StateVector(n) as sv:
+        ref = adjoint_grad(sv, circ, idx, pc.nparams, terms, 0, fused)
+        runs = [adjoint_grad(sv, circ, idx, pc.nparams, terms, c, fused) for c in (0, 5, 2, 0)]
+        z0 = np.zeros(1 << n, complex)
+        z0[0] = 1
+        assert abs(expval(sv, terms) - oracle.pauli_expval(z0, n, terms)) < 1e-12   # shares the accumulator
+        sv.release_workspace()
+        runs.append(adjoint_grad(sv, circ, idx, pc.nparams, terms, 3, fused))
+        sv.release_workspace()
+        sv.release_workspace()
+    for ev, g, drift in runs:
+        assert abs(ev - ref[0]) < 1e-12
+        assert np.abs(g - ref[1]).max() < 1e-11
+        assert drift < 1e-12
