@@ -288,7 +288,7 @@ def extra_workloads(args):
     measured against complex128 on the same circuit family at 28 qubits."""
     import numpy as np
     import torch
-    from subquokka_dev_b200 import Plan, StateVector, adjoint_grad, circuits, zz_x_hamiltonian
+    from subquokka_dev_b200 import Circuit, Plan, StateVector, adjoint_grad, circuits, make_gate, zz_x_hamiltonian
     from subquokka_dev_b200.torch_shim import hea_template
     out = {}
     stream = torch.cuda.current_stream().cuda_stream
@@ -385,6 +385,27 @@ def extra_workloads(args):
         p28.close()
     a.close()
     out["random33_c64"] = res33
+
+    # single 6-qubit blocks on a 28-qubit c64 state (2 GiB): one tensor-core
+    # pass each, for qubit sets that own qubit 0 (state as the N operand) or not
+    n28 = 28
+    sv = StateVector(n28, "c64")
+    sv.set_stream(stream)
+    rng = np.random.default_rng(28)
+    lay = {}
+    for qs in ((10, 11, 12, 13, 14, 15), (3, 4, 7, 8, 9, 10), (1, 2, 7, 8, 9, 10), (0, 1, 2, 3, 4, 5),
+               (0, 1, 21, 22, 26, 27)):
+        gates = [make_gate("U1", [q], coeff=circuits.u3_matrix(*rng.uniform(0, 2 * np.pi, 3))) for q in qs]
+        gates += [make_gate("CP", [qs[k], qs[k + 1]], np.pi) for k in range(5)]
+        pb = Plan(Circuit(gates), n28, "c64", fuse_width=6)
+        if pb.stats()[0] != 1:
+            raise RuntimeError("expected one dense block")
+        ms = time_device(lambda: pb.apply(sv), 3, 10)
+        lay[",".join(map(str, qs))] = {"layout": "state_n" if 0 in qs else "state_m", "ms_per_pass": ms,
+                                       "hbm_gbs": 2 * (8 << n28) / (ms / 1e3) / 1e9}
+        pb.close()
+    sv.close()
+    out["tensor_core_blocks_28q"] = lay
 
     # batch of 256 variational circuits (14-22 qubits, 4-16 layers), complex64,
     # forward + <H> + adjoint gradients from one CUDA graph; tile shapes autotuned
