@@ -20,8 +20,9 @@
 // thread holds whole (re, im) pairs of one row, and a warp's stores run along
 // n, the contiguous direction of the state whenever the block does not own
 // qubit 0.  Operands sit in shared memory in the canonical K-major
-// no-swizzle layout: 8-row x 16-byte core matrices, LBO = 128 B between K
-// chunks, SBO = 2048 B between row groups.
+// 128-byte-swizzle layout (rows of 64 K elements, 16-byte chunks XORed with
+// the row index mod 8, SBO = 1024 B between 8-row groups, atoms 1024-byte
+// aligned); an MMA step's descriptor points at its 32 bytes inside the atom.
 //
 // Pipeline per CTA (state operand double-buffered in shared memory, two
 // accumulators in TMEM): convert supertile s into buffer s % 2, issue its
@@ -55,19 +56,26 @@ struct DenseDesc {
     uint32_t blockmask; // tile-local bits that are the block's qubits
 };
 
-// byte offset of element (row r, k) of a K-major bf16 operand with 128 K columns
-__host__ __device__ __forceinline__ uint32_t kmajor_off(uint32_t r, uint32_t k) {
-    return (r >> 3) * 2048u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+// Byte offset of element (row r, k) of a 128-row x 128-K bf16 operand in the
+// canonical K-major 128-byte-swizzle layout: two K atoms of 64 elements (16 KB
+// each, row r at 128 r), the 16-byte chunk index XORed with r % 8 so that
+// eight rows' chunks at one K fall into different banks.
+__host__ __device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t k) {
+    return (k >> 6) * 16384u + r * 128u + ((((k >> 3) & 7u) ^ (r & 7u)) << 4) + (k & 7u) * 2u;
 }
 
 __device__ __forceinline__ uint32_t s_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;   // leading byte offset: next K chunk
-    d |= (uint64_t)((2048u >> 4) & 0x3FFFu) << 32;  // stride byte offset: next 8-row group
-    d |= (uint64_t)1 << 46;                         // descriptor version (sm_100)
-    return d;                                       // base offset 0, no swizzle
+// Shared-memory descriptor of MMA step kk (K = 16 kk .. 16 kk + 15) of an
+// operand at saddr (1024-byte aligned): the step's 32 bytes inside its atom.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, int kk) {
+    const uint32_t a = saddr + (uint32_t)(kk >> 2) * 16384u + (uint32_t)(kk & 3) * 32u;
+    uint64_t d = (uint64_t)((a >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                          // leading byte offset: unused (swizzled K-major)
+    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;   // stride byte offset: next 8-row group
+    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                          // 128-byte swizzle
+    return d;
 }
 
 // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
@@ -131,6 +139,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
     unsigned char *Wl = Wh + kTcOpBytes;
     unsigned char *S0 = Wl + kTcOpBytes;    // buffer b: hi at S0 + 2b op, lo after it
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (s_u32(sm) & 1023u) {   // the swizzle pattern needs 1024-byte aligned operands
+        if (tid == 0) atomicExch(err, 2);
+        return;
+    }
 
     for (uint32_t i = tid; i < 2 * kTcOpBytes / 16; i += kTcThreads)
         reinterpret_cast<uint4 *>(Wh)[i] = reinterpret_cast<const uint4 *>(gW)[i];
@@ -232,10 +244,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
         if constexpr (!STATE_N) {
             if (!active) return;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) chunk(x + 4 * c, Sh, Sl, kmajor_off(n_m, 2 * (16 * cg_m + 4 * c)));
+            for (int c = 0; c < 4; ++c) chunk(x + 4 * c, Sh, Sl, sw128_off(n_m, 2 * (16 * cg_m + 4 * c)));
         } else {
 #pragma unroll
-            for (int u = 0; u < NU; ++u) chunk(x + 4 * u, Sh, Sl, kmajor_off(conv_n | (u << 5), 8 * conv_c));
+            for (int u = 0; u < NU; ++u) chunk(x + 4 * u, Sh, Sl, sw128_off(conv_n | (u << 5), 8 * conv_c));
         }
     };
     auto issue = [&](const unsigned char *Sh, const unsigned char *Sl, uint32_t acc_col, uint64_t *b) {
@@ -244,7 +256,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
             const uint32_t sa = s_u32(sp == 1 ? Sl : Sh), w = s_u32(sp == 2 ? Wl : Wh);
 #pragma unroll 1
             for (int kk = 0; kk < 8; ++kk) {
-                const uint64_t sd = umma_desc(sa + kk * 256), wd = umma_desc(w + kk * 256);
+                const uint64_t sd = umma_desc(sa, kk), wd = umma_desc(w, kk);
                 const uint64_t ad = STATE_N ? wd : sd, bd = STATE_N ? sd : wd;
                 const uint32_t acc = (sp | kk) ? 1u : 0u;
                 asm volatile(
@@ -416,7 +428,7 @@ void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out) {
                     const float x = (float)v[a][c];
                     const uint16_t h = bf16_rn(x);
                     const uint16_t l = bf16_rn((float)(v[a][c] - (double)bf16_to_f(h)));
-                    const uint32_t off = kmajor_off(2 * ip + a, 2 * i + c);
+                    const uint32_t off = sw128_off(2 * ip + a, 2 * i + c);
                     std::memcpy(hi + off, &h, 2);
                     std::memcpy(lo + off, &l, 2);
                 }

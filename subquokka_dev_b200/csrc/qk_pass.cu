@@ -467,6 +467,7 @@ int qk_plan_apply(qk_sv *sv, qk_plan *p) {
         e = cudaMemcpyAsync(&herr, p->derr, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_err(e, "dense blocks");
+        if (herr == 2) return fail(QK_ERR_CUDA, "tensor-core pass: shared memory not 1024-byte aligned");
         if (herr) return fail(QK_ERR_CUDA, "a tensor-core pass gave up waiting for its contraction");
         return QK_OK;
     }
