@@ -43,7 +43,8 @@
 
 namespace qk {
 
-constexpr int kTcThreads = 512;
+constexpr int kTcDataWarps = 16;                     // load, convert, drain
+constexpr int kTcThreads = 32 * (kTcDataWarps + 1);   // + one MMA-issuer warp
 constexpr int kTcMaxTileBits = 13;                    // 64 x 128 amplitudes
 constexpr int kTcMinTileBits = 12;                    // 64 x 64
 constexpr uint32_t kTcOpBytes = 128 * 128 * 2;        // one 128 x 128 bf16 operand
@@ -132,13 +133,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
                                                             const __grid_constant__ DenseDesc dd,
                                                             const uint16_t *__restrict__ gW, int *__restrict__ err) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t bar[2];
+    // full[b]: buffer b converted (one arrival per data warp); mma[b]: the
+    // contraction of buffer b done (tcgen05.commit); empty[b]: accumulator b
+    // drained (one arrival per data warp)
+    __shared__ __align__(8) uint64_t full[2], mma[2], empty[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ volatile int bad_s;
     const PassDesc &d = dd.p;
     unsigned char *Wh = sm;
     unsigned char *Wl = Wh + kTcOpBytes;
     unsigned char *S0 = Wl + kTcOpBytes;    // buffer b: hi at S0 + 2b op, lo after it
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool issuer = warp == kTcDataWarps;
     if (s_u32(sm) & 1023u) {   // the swizzle pattern needs 1024-byte aligned operands
         if (tid == 0) atomicExch(err, 2);
         return;
@@ -150,251 +156,258 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
         for (uint32_t i = tid; i < 4 * kTcOpBytes / 16; i += kTcThreads)
             reinterpret_cast<uint4 *>(S0)[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&bar[0])), "r"(1) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&bar[1])), "r"(1) : "memory");
+        bad_s = 0;
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&full[b])), "r"(kTcDataWarps) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&mma[b])), "r"(1) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&empty[b])), "r"(kTcDataWarps) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (issuer) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_u32(&tmem_slot)),
                      "r"(kTcTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
 
-    // state offsets of the tile's index bits: jn(n) for the other index,
-    // jb(i) for the block index (both linear in the bits)
+    // data warps: this thread's state row n and block indices 16 cg .. 16 cg + 15
+    // (STATE_M: loads, conversion and, as TMEM lane n / columns 32 cg .., the
+    // drain), offset of amplitude k = lrow + sum of le[b], b in bits(k);
+    // STATE_N: load chunk u at lrow + lu[u] (+ lpair for its second pair),
+    // drain lane at drow + sum of de[b] over the bits of its column index
     const uint32_t tmask = (1u << d.T) - 1, nmask = tmask & ~dd.blockmask;
     auto jn = [&](uint32_t v) { return pass_off(deposit_bits(v, nmask), d); };
     auto jb = [&](uint32_t v) { return pass_off(deposit_bits(v, dd.blockmask), d); };
-
-    // STATE_M: row n, offset of amplitude k = lrow + sum of le[b], b in bits(k)
-    // STATE_N: load chunk u at lrow + lu[u] (+ lpair for its second pair);
-    //          drain lane: row drow, column k at drow + sum of de[b], b in bits(k)
-    uint32_t n_m = 0, cg_m = 0;
+    uint32_t n_m = 0, cg_m = 0, conv_n = 0, conv_c = 0;
     bool active = true;
     uint64_t lrow = 0, le[4] = {0, 0, 0, 0}, lu[2] = {0, 0}, lpair = 0, drow = 0, de[4] = {0, 0, 0, 0};
-    uint32_t conv_n = 0, conv_c = 0;
-    if constexpr (!STATE_N) {
-        n_m = tid & 127;
-        cg_m = tid >> 7;
-        active = n_m < NROWS;
-        lrow = jn(n_m) + jb(16 * cg_m);
+    if (!issuer) {
+        if constexpr (!STATE_N) {
+            n_m = tid & 127;
+            cg_m = tid >> 7;
+            active = n_m < NROWS;
+            lrow = jn(n_m) + jb(16 * cg_m);
 #pragma unroll
-        for (int b = 0; b < 4; ++b) le[b] = jb(1u << b);
-    } else {
-        // chunk (n, c), n = (t & 7) | ((t >> 7) & 3) << 3 | u << 5, c = (t >> 3) & 15
-        conv_n = (tid & 7) | (((tid >> 7) & 3) << 3);
-        conv_c = (tid >> 3) & 15;
-        lrow = jn(conv_n) + jb(4 * conv_c);
-        lu[0] = jn(32);
-        lu[1] = jn(64);
-        lpair = jb(2);
-        // drain: lanes m = 32 (warp % 4) + lane, columns 32 (warp / 4) + 16 h + 2 j + (lane & 1)
-        drow = jb(16 * (warp & 3) + (lane >> 1)) + jn(32 * (warp >> 2) + (lane & 1));
+            for (int b = 0; b < 4; ++b) le[b] = jb(1u << b);
+        } else {
+            // chunk (n, c), n = (t & 7) | ((t >> 7) & 3) << 3 | u << 5, c = (t >> 3) & 15
+            conv_n = (tid & 7) | (((tid >> 7) & 3) << 3);
+            conv_c = (tid >> 3) & 15;
+            lrow = jn(conv_n) + jb(4 * conv_c);
+            lu[0] = jn(32);
+            lu[1] = jn(64);
+            lpair = jb(2);
+            // drain: lanes m = 32 (warp % 4) + lane, columns 32 (warp / 4) + 16 h + 2 j + (lane & 1)
+            drow = jb(16 * (warp & 3) + (lane >> 1)) + jn(32 * (warp >> 2) + (lane & 1));
 #pragma unroll
-        for (int b = 0; b < 4; ++b) de[b] = jn(2u << b);
+            for (int b = 0; b < 4; ++b) de[b] = jn(2u << b);
+        }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    constexpr int NU = STATE_N ? NROWS / 32 : 4;   // STATE_N: chunks per thread
 
-    auto load = [&](float2 (&x)[16], const float2 *p) {
-        if constexpr (!STATE_N) {
-            if (active) {
-                const float2 *q[16];
-                q[0] = p + lrow;
-#pragma unroll
-                for (int k = 1; k < 16; ++k) q[k] = q[k & (k - 1)] + le[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
-#pragma unroll
-                for (int k = 0; k < 16; ++k) x[k] = *q[k];
-            }
-        } else {
-#pragma unroll
-            for (int u = 0; u < NU; ++u) {
-                const float2 *q = p + lrow + (u & 1 ? lu[0] : 0) + (u & 2 ? lu[1] : 0);
-                const float4 v0 = *reinterpret_cast<const float4 *>(q);
-                const float4 v1 = *reinterpret_cast<const float4 *>(q + lpair);
-                x[4 * u + 0] = make_float2(v0.x, v0.y);
-                x[4 * u + 1] = make_float2(v0.z, v0.w);
-                x[4 * u + 2] = make_float2(v1.x, v1.y);
-                x[4 * u + 3] = make_float2(v1.z, v1.w);
-            }
-        }
-    };
-    // four amplitudes (consecutive block indices) -> one 16-byte hi and lo chunk
-    auto chunk = [&](const float2 *x4, unsigned char *Sh, unsigned char *Sl, uint32_t o) {
-        float hi[8], lo[8];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float xs[2] = {x4[q].x, x4[q].y};
-#pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const float h = __bfloat162float(__float2bfloat16_rn(xs[b]));
-                hi[2 * q + b] = h;
-                lo[2 * q + b] = xs[b] - h;
-            }
-        }
-        store_bf16x8(Sh + o, hi);
-        store_bf16x8(Sl + o, lo);
-    };
-    auto convert = [&](const float2 (&x)[16], unsigned char *Sh, unsigned char *Sl) {
-        if constexpr (!STATE_N) {
-            if (!active) return;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) chunk(x + 4 * c, Sh, Sl, sw128_off(n_m, 2 * (16 * cg_m + 4 * c)));
-        } else {
-#pragma unroll
-            for (int u = 0; u < NU; ++u) chunk(x + 4 * u, Sh, Sl, sw128_off(conv_n | (u << 5), 8 * conv_c));
-        }
-    };
-    auto issue = [&](const unsigned char *Sh, const unsigned char *Sl, uint32_t acc_col, uint64_t *b) {
-#pragma unroll 1
-        for (int sp = 0; sp < 3; ++sp) {   // S W products: hi hi, lo hi, hi lo
-            const uint32_t sa = s_u32(sp == 1 ? Sl : Sh), w = s_u32(sp == 2 ? Wl : Wh);
-#pragma unroll 1
-            for (int kk = 0; kk < 8; ++kk) {
-                const uint64_t sd = umma_desc(sa, kk), wd = umma_desc(w, kk);
-                const uint64_t ad = STATE_N ? wd : sd, bd = STATE_N ? sd : wd;
-                const uint32_t acc = (sp | kk) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-                        tmem + acc_col),
-                    "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-                    : "memory");
-            }
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_u32(b))
-                     : "memory");
-    };
-    auto tmem_ld16 = [&](uint32_t taddr, uint32_t (&r)[16]) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-            "%13, %14, %15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    };
-    auto drain = [&](uint32_t acc_col, float2 *p) {
-        const uint32_t lane_base = tmem + ((32u * (uint32_t)(warp & 3)) << 16) + acc_col + 32u * (uint32_t)(warp >> 2);
-        if constexpr (!STATE_N) {
-            // two 16-column halves (8 amplitudes each) of row n
-            float2 *q[16];
-            q[0] = p + lrow;
-#pragma unroll
-            for (int k = 1; k < 16; ++k) q[k] = q[k & (k - 1)] + le[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint32_t r[16];
-                tmem_ld16(lane_base + 16u * h, r);
-                if (active) {
-#pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                        *q[8 * h + k] = make_float2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1]));
+    if (issuer) {
+        // one thread issues every contraction: wait until buffer b is
+        // converted and accumulator b drained, then 24 MMAs and a commit
+        if (lane == 0) {
+            uint32_t it = 0;
+            for (uint64_t o = blockIdx.x; o < nsup && !bad_s; o += gridDim.x, ++it) {
+                const uint32_t b = it & 1;
+                if (!tc_wait(&full[b], (it >> 1) & 1u) || (it >= 2 && !tc_wait(&empty[b], ((it - 2) >> 1) & 1u))) {
+                    bad_s = 1;
+                    break;
                 }
-            }
-        } else {
-            // lane holds one of re/im of block index i' for 32 columns n;
-            // after the swap, lane (re) stores even n, lane (im) odd n
-            const uint32_t comp = lane & 1;
-            float2 *q[16];
-            q[0] = p + drow;
-#pragma unroll
-            for (int k = 1; k < 16; ++k) q[k] = q[k & (k - 1)] + de[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint32_t r[16];
-                tmem_ld16(lane_base + 16u * h, r);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const float keep = __uint_as_float(comp ? r[2 * j + 1] : r[2 * j]);
-                    const float send = __uint_as_float(comp ? r[2 * j] : r[2 * j + 1]);
-                    const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
-                    if (32 * (warp >> 2) + 16 * h + 2 * j < NROWS)
-                        *q[8 * h + j] = comp ? make_float2(recv, keep) : make_float2(keep, recv);
-                }
-            }
-        }
-    };
-
-    // Each warp waits for a contraction on its own (lane 0 polls, bounded);
-    // a timeout is recorded in bad_s and seen by every thread after the next
-    // CTA barrier, so all threads leave the loop together.
-    __shared__ int bad_s;
-    if (tid == 0) bad_s = 0;
-    auto wait_warp = [&](uint64_t *bb, uint32_t parity) -> uint32_t {
-        uint32_t dn = 0;
-        if (lane == 0) dn = tc_wait(bb, parity);
-        return __shfl_sync(0xffffffffu, dn, 0);
-    };
-
-    // one supertile: convert x (supertile o) into buffer it % 2, start its
-    // contraction, refill x with supertile o + 2 grid, drain supertile it - 1
-    uint32_t it = 0;
-    bool bad = false;
-    float2 *prev = s;
-    auto step = [&](float2 (&x)[16], uint64_t o) {
-        const uint32_t b = it & 1;
-        unsigned char *Sh = S0 + 2 * b * kTcOpBytes, *Sl = Sh + kTcOpBytes;
-        // buffer b and accumulator b were released by this warp's wait and
-        // drain of supertile it - 2 (and every warp's, by the barrier below)
-        convert(x, Sh, Sl);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (bad_s) {
-            bad = true;
-            return;
-        }
-        if (tid == 0) issue(Sh, Sl, b * 128u, &bar[b]);
-        __syncwarp();   // warp 0 reconverges before its aligned tcgen05 ops
-        if (o + 2ull * gridDim.x < nsup) load(x, s + pass_base(o + 2ull * gridDim.x, d));
-        if (it > 0) {
-            const uint32_t pb = b ^ 1u;
-            if (wait_warp(&bar[pb], ((it - 1) >> 1) & 1u)) {
                 tc_fence_after();
-                drain(pb * 128u, prev);
+                const unsigned char *Sh = S0 + 2 * b * kTcOpBytes, *Sl = Sh + kTcOpBytes;
+#pragma unroll 1
+                for (int sp = 0; sp < 3; ++sp) {   // S W products: hi hi, lo hi, hi lo
+                    const uint32_t sa = s_u32(sp == 1 ? Sl : Sh), w = s_u32(sp == 2 ? Wl : Wh);
+#pragma unroll 1
+                    for (int kk = 0; kk < 8; ++kk) {
+                        const uint64_t sd = umma_desc(sa, kk), wd = umma_desc(w, kk);
+                        const uint64_t ad = STATE_N ? wd : sd, bd = STATE_N ? sd : wd;
+                        const uint32_t acc = (sp | kk) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                tmem + b * 128u),
+                            "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                            : "memory");
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 s_u32(&mma[b]))
+                             : "memory");
+            }
+        }
+        __syncwarp();   // the issuer warp reaches the final barrier converged
+    } else {
+        auto load = [&](float2 (&x)[16], const float2 *p) {
+            if constexpr (!STATE_N) {
+                if (active) {
+                    const float2 *q[16];
+                    q[0] = p + lrow;
+#pragma unroll
+                    for (int k = 1; k < 16; ++k)
+                        q[k] = q[k & (k - 1)] + le[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) x[k] = *q[k];
+                }
+            } else {
+                constexpr int NU = NROWS / 32;   // chunks per thread
+#pragma unroll
+                for (int u = 0; u < NU; ++u) {
+                    const float2 *q = p + lrow + (u & 1 ? lu[0] : 0) + (u & 2 ? lu[1] : 0);
+                    const float4 v0 = *reinterpret_cast<const float4 *>(q);
+                    const float4 v1 = *reinterpret_cast<const float4 *>(q + lpair);
+                    x[4 * u + 0] = make_float2(v0.x, v0.y);
+                    x[4 * u + 1] = make_float2(v0.z, v0.w);
+                    x[4 * u + 2] = make_float2(v1.x, v1.y);
+                    x[4 * u + 3] = make_float2(v1.z, v1.w);
+                }
+            }
+        };
+        // four amplitudes (consecutive block indices) -> one 16-byte hi and lo chunk
+        auto chunk = [&](const float2 *x4, unsigned char *Sh, unsigned char *Sl, uint32_t o) {
+            float hi[8], lo[8];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float xs[2] = {x4[q].x, x4[q].y};
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const float h = __bfloat162float(__float2bfloat16_rn(xs[b]));
+                    hi[2 * q + b] = h;
+                    lo[2 * q + b] = xs[b] - h;
+                }
+            }
+            store_bf16x8(Sh + o, hi);
+            store_bf16x8(Sl + o, lo);
+        };
+        auto convert = [&](const float2 (&x)[16], unsigned char *Sh, unsigned char *Sl) {
+            if constexpr (!STATE_N) {
+                if (!active) return;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) chunk(x + 4 * c, Sh, Sl, sw128_off(n_m, 2 * (16 * cg_m + 4 * c)));
+            } else {
+#pragma unroll
+                for (int u = 0; u < NROWS / 32; ++u)
+                    chunk(x + 4 * u, Sh, Sl, sw128_off(conv_n | (u << 5), 8 * conv_c));
+            }
+        };
+        auto tmem_ld16 = [&](uint32_t taddr, uint32_t (&r)[16]) {
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        };
+        auto drain = [&](uint32_t acc_col, float2 *p) {
+            const uint32_t lane_base =
+                tmem + ((32u * (uint32_t)(warp & 3)) << 16) + acc_col + 32u * (uint32_t)(warp >> 2);
+            float2 *q[16];
+            q[0] = p + (STATE_N ? drow : lrow);
+#pragma unroll
+            for (int k = 1; k < 16; ++k)
+                q[k] = q[k & (k - 1)] + (STATE_N ? de : le)[(k & 1) ? 0 : (k & 2) ? 1 : (k & 4) ? 2 : 3];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t r[16];
+                tmem_ld16(lane_base + 16u * h, r);
+                if constexpr (!STATE_N) {
+                    // row n: 8 amplitudes (re, im adjacent columns)
+                    if (active) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k)
+                            *q[8 * h + k] = make_float2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1]));
+                    }
+                } else {
+                    // one of re/im of block index i' for 16 columns n; after
+                    // the swap, lane (re) stores even n, lane (im) odd n
+                    const uint32_t comp = lane & 1;
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float keep = __uint_as_float(comp ? r[2 * j + 1] : r[2 * j]);
+                        const float send = __uint_as_float(comp ? r[2 * j] : r[2 * j + 1]);
+                        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+                        if (32 * (warp >> 2) + 16 * h + 2 * j < NROWS)
+                            *q[8 * h + j] = comp ? make_float2(recv, keep) : make_float2(keep, recv);
+                    }
+                }
+            }
+        };
+        auto wait_warp = [&](uint64_t *bb, uint32_t parity) -> uint32_t {
+            uint32_t dn = 0;
+            if (lane == 0) dn = tc_wait(bb, parity);
+            return __shfl_sync(0xffffffffu, dn, 0);
+        };
+        auto arrive = [&](uint64_t *bb) {
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s_u32(bb)) : "memory");
+        };
+
+        // per supertile: convert x (supertile o) into buffer it % 2 and hand
+        // it to the issuer, refill x with supertile o + grid, then drain the
+        // contraction of supertile it - 1
+        uint32_t it = 0;
+        bool bad = false;
+        float2 x[16];
+        uint64_t o = blockIdx.x, base = 0, prev = 0;
+        if (o < nsup) {
+            base = pass_base(o, d);
+            load(x, s + base);
+        }
+        for (; o < nsup; o += gridDim.x, ++it) {
+            if (__shfl_sync(0xffffffffu, bad_s, 0)) {
+                bad = true;
+                break;
+            }
+            const uint32_t b = it & 1;
+            unsigned char *Sh = S0 + 2 * b * kTcOpBytes, *Sl = Sh + kTcOpBytes;
+            // buffer b was released by this warp's wait for contraction it - 2
+            convert(x, Sh, Sl);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            arrive(&full[b]);
+            const uint64_t cur = base;
+            if (o + gridDim.x < nsup) {
+                base = pass_base(o + gridDim.x, d);
+                load(x, s + base);
+            }
+            if (it > 0) {
+                const uint32_t pb = b ^ 1u;
+                if (!wait_warp(&mma[pb], ((it - 1) >> 1) & 1u)) {
+                    if (lane == 0) bad_s = 1;
+                    bad = true;
+                    break;
+                }
+                tc_fence_after();
+                drain(pb * 128u, s + prev);
+                tc_fence_before();
+                arrive(&empty[pb]);
+            }
+            prev = cur;
+        }
+        if (!bad && it > 0) {
+            const uint32_t pb = (it - 1) & 1u;
+            if (wait_warp(&mma[pb], ((it - 1) >> 1) & 1u)) {
+                tc_fence_after();
+                drain(pb * 128u, s + prev);
             } else if (lane == 0) {
                 bad_s = 1;
             }
-            tc_fence_before();
-        }
-        prev = s + pass_base(o, d);
-        ++it;
-    };
-
-    float2 xa[16], xb[16];
-    uint64_t o = blockIdx.x;
-    if (o < nsup) load(xa, s + pass_base(o, d));
-    if (o + gridDim.x < nsup) load(xb, s + pass_base(o + gridDim.x, d));
-    while (o < nsup) {
-        step(xa, o);
-        o += gridDim.x;
-        if (bad || o >= nsup) break;
-        step(xb, o);
-        o += gridDim.x;
-        if (bad) break;
-    }
-    if (!bad && it > 0) {
-        const uint32_t pb = (it - 1) & 1u;
-        if (wait_warp(&bar[pb], ((it - 1) >> 1) & 1u)) {
-            tc_fence_after();
-            drain(pb * 128u, prev);
-        } else if (lane == 0) {
-            bad_s = 1;
         }
     }
-    __syncthreads();
-    if (bad_s && tid == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+    if (bad_s && tid == 0) atomicExch(err, 1);
+    if (issuer) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
 }
 
 // ---- host side ----------------------------------------------------------------

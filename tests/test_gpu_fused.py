@@ -143,3 +143,42 @@ def test_tensor_core_random_circuit_family():
     ref = oracle.apply_circuit(zero(n), n, circ)
     out = run_plan(n, circ, None, "c64", fuse_width=6)
     assert fidelity_err(out, ref) <= 1e-6
+
+
+def block_circuit(blocks, seed):
+    """Gates that the fuser groups into exactly the given 6-qubit blocks."""
+    rng = np.random.default_rng(seed)
+    gates = []
+    for qs in blocks:
+        qs = sorted(qs)
+        for a, b in zip(qs, qs[1:]):
+            gates.append(make_gate("CP", [a, b], float(rng.uniform(0, 6))))
+        for q in qs:
+            gates.append(make_gate("U1", [q], coeff=circuits.u3_matrix(*rng.uniform(0, 2 * np.pi, 3))))
+        for a, b in zip(qs, qs[1:]):
+            gates.append(make_gate("CP", [a, b], float(rng.uniform(0, 6))))
+    return Circuit(gates)
+
+
+@pytest.mark.parametrize("n,blocks", [
+    (16, [[0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11]]),          # first block owns qubit 0
+    (16, [[6, 7, 8, 9, 10, 11], [0, 1, 2, 3, 4, 5]]),          # second block owns qubit 0
+    (16, [[0, 1, 2, 8, 9, 10], [0, 3, 4, 5, 12, 13]]),         # both, overlapping
+    (16, [[3, 4, 5, 6, 7, 8], [9, 10, 11, 12, 13, 14]]),       # neither
+    (16, [[2, 5, 7, 9, 11, 13], [1, 4, 6, 8, 10, 15]]),        # interleaved qubits
+    (13, [[1, 2, 3, 4, 5, 6], [7, 8, 9, 10, 11, 12]]),         # one supertile
+    (15, [[0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11], [3, 4, 5, 12, 13, 14]]),  # a pair and a single
+])
+def test_tensor_core_block_pairs(n, blocks):
+    # consecutive blocks run as one pass (two contractions per supertile, the
+    # first result transposed into the second operand in shared memory)
+    circ = block_circuit(blocks, 7 + n)
+    p = Plan(circ, n, "c64", fuse_width=6)
+    got = [p.dense_block(k)[0] for k in range(p.stats()[0])]
+    assert len(got) == len(blocks) and got[:2] == blocks[:2]
+    p.close()
+    init = circuits.random_state(n, 8)
+    ref = oracle.apply_circuit(init, n, circ)
+    out = run_plan(n, circ, init, "c64", fuse_width=6)
+    assert fidelity_err(out, ref) <= 1e-6
+    assert np.abs(out - ref).max() <= 5e-5
