@@ -169,9 +169,10 @@ def block_circuit(blocks, seed):
     (13, [[1, 2, 3, 4, 5, 6], [7, 8, 9, 10, 11, 12]]),         # one supertile
     (15, [[0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11], [3, 4, 5, 12, 13, 14]]),  # a pair and a single
 ])
-def test_tensor_core_block_pairs(n, blocks):
-    # consecutive blocks run as one pass (two contractions per supertile, the
-    # first result transposed into the second operand in shared memory)
+def test_tensor_core_block_sequences(n, blocks):
+    # blocks on chosen qubit sets: both operand layouts (qubit 0 in the first,
+    # the second, both or neither block), interleaved qubits, a 13-qubit
+    # state (one supertile) and a trailing block
     circ = block_circuit(blocks, 7 + n)
     p = Plan(circ, n, "c64", fuse_width=6)
     got = [p.dense_block(k)[0] for k in range(p.stats()[0])]
