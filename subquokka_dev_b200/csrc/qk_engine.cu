@@ -128,6 +128,9 @@ static int launch_op(C *s, int n, const Op &op, cudaStream_t st) {
         k_swap2<C><<<sweep_blocks(namp / 4), kBlock, 0, st>>>(s, namp / 4, a, b);
         break;
     }
+    case OP_CX:
+        k_cx<C><<<sweep_blocks(namp / 4), kBlock, 0, st>>>(s, namp / 4, op.q[op.aux], op.q[1 - op.aux]);
+        break;
     case OP_PERM:
         // a VSWAP is a pure permutation: a tile pass over the swapped qubits
         // writes each tile back permuted, reads and writes stay coalesced

@@ -213,6 +213,34 @@ __global__ void __launch_bounds__(kBlock) k_diag2(C *__restrict__ s, uint64_t na
 }
 
 // Exchange |..1..0..> and |..0..1..> of qubits qa < qb (SWAP): half the state.
+// Controlled X: swap the amplitude pairs of target qt where control qc is
+// set (a quarter of the amplitudes are read and written twice over: S bytes).
+template <typename C>
+__global__ void __launch_bounds__(kBlock) k_cx(C *__restrict__ s, uint64_t nquads, int qc, int qt) {
+    const uint64_t p0 = item0();
+    const int lo = qc < qt ? qc : qt, hi = qc < qt ? qt : qc;
+    const uint64_t Cb = 1ull << qc, Tb = 1ull << qt;
+    C a[kUnroll], b[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        const uint64_t p = p0 + (uint64_t)u * kBlock;
+        if (p < nquads) {
+            const uint64_t i = ins0(ins0(p, lo), hi) | Cb;
+            a[u] = s[i];
+            b[u] = s[i | Tb];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        const uint64_t p = p0 + (uint64_t)u * kBlock;
+        if (p < nquads) {
+            const uint64_t i = ins0(ins0(p, lo), hi) | Cb;
+            s[i] = b[u];
+            s[i | Tb] = a[u];
+        }
+    }
+}
+
 template <typename C>
 __global__ void __launch_bounds__(kBlock) k_swap2(C *__restrict__ s, uint64_t nquads, int qa, int qb) {
     const uint64_t p0 = item0();

@@ -187,6 +187,33 @@ int lower_gate(const qk_gate &g, Op &op) {
             op.m[2 * i] = g.coeff[2 * res];
             op.m[2 * i + 1] = g.coeff[2 * res + 1];
         }
+        // A matrix of exact 0 / 1 entries that is a CNOT or SWAP, or any
+        // diagonal matrix, runs as that cheaper op.  The reference's dense
+        // product with these entries gives the same amplitudes (up to the
+        // sign of zeros).
+        auto permutation = [&](const int (&row)[4]) {   // row[c]: row of column c's 1
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c)
+                    if (op.m[2 * (4 * r + c)] != (row[c] == r ? 1.0 : 0.0) || op.m[2 * (4 * r + c) + 1] != 0.0)
+                        return false;
+            return true;
+        };
+        static const int cx0[4] = {0, 3, 2, 1}, cx1[4] = {0, 1, 3, 2}, swp[4] = {0, 2, 1, 3};
+        bool diagonal = true;
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c)
+                if (r != c && (op.m[2 * (4 * r + c)] != 0.0 || op.m[2 * (4 * r + c) + 1] != 0.0)) diagonal = false;
+        if (permutation(cx0) || permutation(cx1)) {
+            op.aux = permutation(cx0) ? 0 : 1;   // control q[aux], target q[1 - aux]
+            op.kind = OP_CX;
+        } else if (permutation(swp)) {
+            op.kind = OP_SWAP2;
+        } else if (diagonal) {
+            double dm[8];
+            for (int k = 0; k < 4; ++k) { dm[2 * k] = op.m[2 * (5 * k)]; dm[2 * k + 1] = op.m[2 * (5 * k) + 1]; }
+            op.kind = OP_DIAG2;
+            std::memcpy(op.m, dm, sizeof dm);
+        }
         return QK_OK;
     }
     case QK_GATE_SWAP:  // SWAPGate: exchange |01> and |10> (src/circuit.cpp:351-355)
@@ -484,6 +511,10 @@ int qk_gate_matrix(const qk_gate *g, double *out, int *dim) {
         for (int k = 0; k < 4; ++k) put(k, k, op.m[2 * k], op.m[2 * k + 1]);
         break;
     case OP_SWAP2: put(0, 0, 1, 0); put(1, 2, 1, 0); put(2, 1, 1, 0); put(3, 3, 1, 0); break;
+    case OP_CX:
+        if (op.aux == 0) { put(0, 0, 1, 0); put(3, 1, 1, 0); put(2, 2, 1, 0); put(1, 3, 1, 0); }
+        else { put(0, 0, 1, 0); put(1, 1, 1, 0); put(3, 2, 1, 0); put(2, 3, 1, 0); }
+        break;
     case OP_PERM: {
         const int k = nq / 2;
         for (int c = 0; c < d; ++c) {

@@ -61,6 +61,22 @@ __device__ __forceinline__ void reg_g1(C (&v)[R], const C m0, const C m1, const 
     }
 }
 
+// Controlled X on register slot S: swap the pair (k, k | 2^S) where bit k of
+// M (the control's value at register index k) is set.
+template <int S, typename C, int R>
+__device__ __forceinline__ void reg_cx(C (&v)[R], uint32_t M) {
+    if constexpr ((1 << S) < R) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (k & (1 << S)) continue;
+            const bool f = (M >> k) & 1;
+            const C a = v[k], b = v[k | (1 << S)];
+            v[k] = f ? b : a;
+            v[k | (1 << S)] = f ? a : b;
+        }
+    }
+}
+
 template <int A, int B, typename C, int R>
 __device__ __forceinline__ void reg_g2(C (&v)[R], const C *__restrict__ m) {
     if constexpr (A < B && (1 << B) < R) {
@@ -295,6 +311,19 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
                 const C ph = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
                 v[kk] = cmul(v[kk], ph);
                 if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
+            }
+            break;
+        }
+        case TOP_CX: {
+            const uint32_t M = bit_set<LOG2R>(op.b, 1, base, tb, bm);
+            switch (op.a) {
+#define QK_CX(S)                                   \
+    case S:                                        \
+        reg_cx<S>(v, M);                           \
+        if constexpr (NS == 2) reg_cx<S>(w, M);    \
+        break;
+            QK_CX(0) QK_CX(1) QK_CX(2) QK_CX(3) QK_CX(4)
+#undef QK_CX
             }
             break;
         }

@@ -69,6 +69,7 @@ size_t op_cost(const Op &op, int dtype) {
     size_t ncoef = 4;
     if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2) ncoef = 16;
     else if (op.kind == OP_PHASE1 || op.kind == OP_PHASE2) ncoef = 1;
+    else if (op.kind == OP_CX) ncoef = 0;
     else if (op.kind == OP_GRAD) return (16 + 8) * 5 / 4;  // one double accumulator
     return (16 + ncoef * c) * 5 / 4;
 }
@@ -121,11 +122,10 @@ struct PassBuilder {
                     if (done[i] || !ready(i)) continue;
                     const Op &op = ops[idx[i]];
                     if (!mapped) continue;  // the first program op is always a TOP_REMAP
-                    if (!op_is_diagonal(op)) {
-                        bool ok = true;
-                        for (int k = 0; k < op.nq; ++k) ok = ok && in_regs(local[op.q[k]]);
-                        if (!ok) continue;
-                    }
+                    bool ok = true;
+                    for (int k = op_reg_first(op); k < op_reg_first(op) + op_reg_count(op); ++k)
+                        ok = ok && in_regs(local[op.q[k]]);
+                    if (!ok) continue;
                     emit(op, local, Q);
                     done[i] = 1;
                     ++ndone;
@@ -141,19 +141,18 @@ struct PassBuilder {
             // following non-diagonal gates in program order
             std::vector<int> nq;
             auto add = [&](const Op &op) {
-                bool fits = true;
+                const int k0 = op_reg_first(op), k1 = k0 + op_reg_count(op);
                 int need = 0;
-                for (int k = 0; k < op.nq; ++k)
+                for (int k = k0; k < k1; ++k)
                     if (std::find(nq.begin(), nq.end(), local[op.q[k]]) == nq.end()) ++need;
-                fits = (int)nq.size() + need <= r;
-                if (!fits) return;
-                for (int k = 0; k < op.nq; ++k)
+                if ((int)nq.size() + need > r) return;
+                for (int k = k0; k < k1; ++k)
                     if (std::find(nq.begin(), nq.end(), local[op.q[k]]) == nq.end()) nq.push_back(local[op.q[k]]);
             };
             for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
-                if (!done[i] && ready(i) && !op_is_diagonal(ops[idx[i]])) add(ops[idx[i]]);
+                if (!done[i] && ready(i) && op_reg_count(ops[idx[i]])) add(ops[idx[i]]);
             for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
-                if (!done[i] && !op_is_diagonal(ops[idx[i]])) add(ops[idx[i]]);
+                if (!done[i] && op_reg_count(ops[idx[i]])) add(ops[idx[i]]);
             for (int b = 0; b < d.T && (int)nq.size() < r; ++b)
                 if (std::find(nq.begin(), nq.end(), b) == nq.end()) nq.push_back(b);
             if (nq.empty()) return fail(QK_ERR_ARG, "planner: no register qubits for a pass");
@@ -231,6 +230,11 @@ struct PassBuilder {
             }
             break;
         }
+        case OP_CX:
+            t.kind = TOP_CX;
+            t.a = (uint8_t)slot(op.q[1 - op.aux]);
+            t.b = code(op.q[op.aux], local);
+            break;
         case OP_PHASE1:
             t.kind = TOP_PHASE;
             t.a = code(op.q[0], local);
@@ -319,13 +323,14 @@ struct PassBuilder {
                 bool blk = false;
                 for (int k = 0; k < op.nq; ++k) blk = blk || blocked[op.q[k]];
                 bool ok = !blk && op.kind != OP_PERM && (take.empty() || used + op_cost(op, plan.dtype) <= budget);
-                if (ok && !op_is_diagonal(op)) {
+                if (ok && op_reg_count(op)) {
+                    const int k0 = op_reg_first(op), k1 = k0 + op_reg_count(op);
                     int need = 0;
-                    for (int k = 0; k < op.nq; ++k)
+                    for (int k = k0; k < k1; ++k)
                         if (std::find(B.begin(), B.end(), op.q[k]) == B.end()) ++need;
                     ok = (int)B.size() + need <= T;
                     if (ok)
-                        for (int k = 0; k < op.nq; ++k)
+                        for (int k = k0; k < k1; ++k)
                             if (std::find(B.begin(), B.end(), op.q[k]) == B.end()) B.push_back(op.q[k]);
                 }
                 if (ok) {
@@ -451,6 +456,10 @@ static void block_apply(std::vector<double> &u, const Op &op, const int *loc) {
     case OP_PHASE2: for (int k = 0; k < 3; ++k) put(k, k, 1, 0); put(3, 3, op.m[0], op.m[1]); break;
     case OP_DIAG2: for (int k = 0; k < 4; ++k) put(k, k, op.m[2 * k], op.m[2 * k + 1]); break;
     case OP_SWAP2: put(0, 0, 1, 0); put(1, 2, 1, 0); put(2, 1, 1, 0); put(3, 3, 1, 0); break;
+    case OP_CX:
+        if (op.aux == 0) { put(0, 0, 1, 0); put(3, 1, 1, 0); put(2, 2, 1, 0); put(1, 3, 1, 0); }
+        else { put(0, 0, 1, 0); put(1, 1, 1, 0); put(3, 2, 1, 0); put(2, 3, 1, 0); }
+        break;
     default: return;
     }
     int mask = 0;
@@ -581,8 +590,7 @@ int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups,
             if (ops[i].kind == OP_PERM) { fits = false; break; }
             used += op_cost(ops[i], o.dtype);
             if (used > program_budget(o.dtype, o.tile_bits, 1)) { fits = false; break; }
-            if (op_is_diagonal(ops[i])) continue;
-            for (int k = 0; k < ops[i].nq; ++k)
+            for (int k = op_reg_first(ops[i]); k < op_reg_first(ops[i]) + op_reg_count(ops[i]); ++k)
                 if (std::find(B.begin(), B.end(), ops[i].q[k]) == B.end()) B.push_back(ops[i].q[k]);
             fits = (int)B.size() <= o.tile_bits;
         }
