@@ -199,6 +199,42 @@ __device__ __forceinline__ uint32_t bit_set(uint8_t code, uint32_t none, uint64_
     return (tb & m) ? 0xFFFFFFFFu : 0u;
 }
 
+// Register slot holding a diagonal-op qubit code, or -1 with *bit set to the
+// qubit's value, which is then the same for every register element.
+template <int LOG2R>
+__device__ __forceinline__ int code_slot(uint8_t code, uint64_t base, uint32_t tb, const uint32_t (&bm)[kPassMaxReg],
+                                         uint32_t *bit) {
+    *bit = 0;
+    if (code == kNoQubit) return -1;
+    if (code & kOuterFlag) {
+        *bit = (uint32_t)(base >> (code & 0x7F)) & 1u;
+        return -1;
+    }
+    const uint32_t m = 1u << code;
+#pragma unroll
+    for (int s = 0; s < LOG2R; ++s)
+        if (bm[s] == m) return s;
+    *bit = (tb & m) ? 1u : 0u;
+    return -1;
+}
+
+// Diagonal phases by register element: element k gets p1 where bit S of k is
+// set, else p0 (S = -1: p0 everywhere).
+template <int S, typename C, int R>
+__device__ __forceinline__ void reg_diag1(C (&v)[R], const C p0, const C p1) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = cmul(v[k], (S >= 0 && (k >> (S < 0 ? 0 : S)) & 1) ? p1 : p0);
+}
+// element k gets d[bit A of k + 2 bit B of k]
+template <int A, int B, typename C, int R>
+__device__ __forceinline__ void reg_diag2(C (&v)[R], const C d0, const C d1, const C d2, const C d3) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int i = ((k >> A) & 1) | (((k >> B) & 1) << 1);
+        v[k] = cmul(v[k], i == 0 ? d0 : i == 1 ? d1 : i == 2 ? d2 : d3);
+    }
+}
+
 // swz index of register element kk under the current mapping
 template <int LOG2R>
 __device__ __forceinline__ uint32_t reg_sidx(int kk, uint32_t stb, const uint32_t (&sb)[LOG2R]) {
@@ -209,24 +245,31 @@ __device__ __forceinline__ uint32_t reg_sidx(int kk, uint32_t stb, const uint32_
     return x;
 }
 
-template <typename C> __device__ __forceinline__ double imdot(C l, C a) { return (double)l.x * a.y - (double)l.y * a.x; }
-template <typename C> __device__ __forceinline__ double redot(C l, C a) { return (double)l.x * a.x + (double)l.y * a.y; }
-
-// Im <lambda|G|psi> over this thread's register pairs of slot S (G = X, Y, Z by gen 1, 2, 3).
+// Im <lambda|G|psi> over this thread's register pairs of slot S (G = X, Y, Z
+// by gen 1, 2, 3), summed in the state's precision (a thread holds at most
+// 16 pairs) and returned as a double for the cross-thread reduction.
 template <int S, typename C, int R>
 __device__ __forceinline__ double reg_grad(const C (&v)[R], const C (&w)[R], int gen) {
-    double s = 0;
+    using T = decltype(v[0].x);
+    T s = 0;
     if constexpr ((1 << S) < R) {
+        auto im = [](C l, C a) { return l.x * a.y - l.y * a.x; };
+        auto re = [](C l, C a) { return l.x * a.x + l.y * a.y; };
+        if (gen == 1) {
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (k & (1 << S)) continue;
-            const C a0 = v[k], a1 = v[k | (1 << S)], l0 = w[k], l1 = w[k | (1 << S)];
-            if (gen == 1) s += imdot(l0, a1) + imdot(l1, a0);
-            else if (gen == 2) s += redot(l1, a0) - redot(l0, a1);
-            else s += imdot(l0, a0) - imdot(l1, a1);
+            for (int k = 0; k < R; ++k)
+                if (!(k & (1 << S))) s += im(w[k], v[k | (1 << S)]) + im(w[k | (1 << S)], v[k]);
+        } else if (gen == 2) {
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                if (!(k & (1 << S))) s += re(w[k | (1 << S)], v[k]) - re(w[k], v[k | (1 << S)]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                if (!(k & (1 << S))) s += im(w[k], v[k]) - im(w[k | (1 << S)], v[k | (1 << S)]);
         }
     }
-    return s;
+    return (double)s;
 }
 
 // Run a pass program on one tile (NS = 1) or on the matching tiles of two
@@ -303,14 +346,43 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             break;
         }
         case TOP_DIAG: {
+            // phases by the two qubits' values: a register-slot qubit varies
+            // over the elements (pattern fixed at compile time), any other is
+            // the same for all of them
             const C d0 = coef[op.coef], d1 = coef[op.coef + 1], d2 = coef[op.coef + 2], d3 = coef[op.coef + 3];
-            const uint32_t A = bit_set<LOG2R>(op.a, 0, base, tb, bm), B = bit_set<LOG2R>(op.b, 0, base, tb, bm);
-#pragma unroll
-            for (int kk = 0; kk < R; ++kk) {
-                const uint32_t idx = ((A >> kk) & 1) | (((B >> kk) & 1) << 1);
-                const C ph = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
-                v[kk] = cmul(v[kk], ph);
-                if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
+            uint32_t ba, bb;
+            const int sa = code_slot<LOG2R>(op.a, base, tb, bm, &ba), sb = code_slot<LOG2R>(op.b, base, tb, bm, &bb);
+            if (sa >= 0 && sb >= 0) {
+                switch (sa * 8 + sb) {
+#define QK_D2(A, B)                                                  \
+    case A * 8 + B:                                                  \
+        reg_diag2<A, B>(v, d0, d1, d2, d3);                          \
+        if constexpr (NS == 2) reg_diag2<A, B>(w, d0, d1, d2, d3);   \
+        break;                                                       \
+    case B * 8 + A:                                                  \
+        reg_diag2<B, A>(v, d0, d1, d2, d3);                          \
+        if constexpr (NS == 2) reg_diag2<B, A>(w, d0, d1, d2, d3);   \
+        break;
+                QK_D2(0, 1) QK_D2(0, 2) QK_D2(0, 3) QK_D2(0, 4) QK_D2(1, 2)
+                QK_D2(1, 3) QK_D2(1, 4) QK_D2(2, 3) QK_D2(2, 4) QK_D2(3, 4)
+#undef QK_D2
+                }
+                break;
+            }
+            // at most one register-slot qubit: two phases p0 / p1 by its value
+            const int sl = sa >= 0 ? sa : sb;
+            C p0, p1;
+            if (sa >= 0) { p0 = bb ? d2 : d0; p1 = bb ? d3 : d1; }
+            else if (sb >= 0) { p0 = ba ? d1 : d0; p1 = ba ? d3 : d2; }
+            else { p0 = p1 = ba ? (bb ? d3 : d1) : (bb ? d2 : d0); }
+            switch (sl) {
+#define QK_D1(S)                                       \
+    case S:                                            \
+        reg_diag1<S>(v, p0, p1);                       \
+        if constexpr (NS == 2) reg_diag1<S>(w, p0, p1); \
+        break;
+            QK_D1(-1) QK_D1(0) QK_D1(1) QK_D1(2) QK_D1(3) QK_D1(4)
+#undef QK_D1
             }
             break;
         }
