@@ -259,7 +259,8 @@ def fused_variants(args, circ, exact, plain_ms, alg):
     from subquokka_dev_b200 import Plan, StateVector
     out = {}
     n = args.qubits
-    for key, dtype, fw in (("c128", "c128", 0), ("c64", "c64", 0), ("c64_tensor_core", "c64", 6)):
+    for key, dtype, fw in (("c128", "c128", 0), ("c64", "c64", 0), ("c64_tensor_core", "c64", 6),
+                           ("c64_tensor_core_width5", "c64", 5)):
         plan = Plan(circ, n, dtype, fuse_width=fw)
         passes, ops, remaps = plan.stats()
         sv = StateVector(n, dtype)

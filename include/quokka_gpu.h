@@ -96,8 +96,8 @@ typedef struct qk_config {
     int32_t MPI_buffe_size;   /* MPI_buffe_size (sic), default 16            */
     int32_t precision;        /* precision=c128|c64 -> qk_dtype, default c128 */
     int32_t fuse_width;       /* fuse_width, default 0: per-gate kernels; on a
-                                 flat circuit > 0 runs fused passes, 6 with
-                                 precision=c64 tensor-core 6-qubit blocks    */
+                                 flat circuit > 0 runs fused passes, 5 or 6
+                                 with precision=c64 tensor-core blocks       */
     int32_t dump_binary;      /* dump_format=bin -> 1, default 0 (text)      */
     char runner_type[32];     /* runner_type, default "IO"; "GPU" selects us */
     char dump_file[256];      /* dump_file, default ""                       */
@@ -203,8 +203,9 @@ typedef struct qk_plan_opts {
                              complex128, 13 for complex64; at most 14)      */
     int32_t reg_bits;     /* qubits held in registers per thread (default 3
                              for complex128, 4 for complex64; at most 5)    */
-    int32_t fuse_width;   /* 0: register passes.  6: gates fused into dense
-                             6-qubit unitaries (FP64 on the host), each
+    int32_t fuse_width;   /* 0: register passes.  5 or 6: gates fused into
+                             dense unitaries on at most that many qubits
+                             (FP64 on the host, padded to 6 qubits), each
                              applied as a 64 x 64 complex contraction on the
                              tensor cores in split precision (3 x BF16, FP32
                              accumulate); complex64 states of >= 12 qubits */
@@ -226,7 +227,7 @@ int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size
                           const qk_plan_opts *opts, qk_plan **out);
 /* Number of passes, program operations and register re-mappings. */
 int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t *remaps);
-/* Block k of a fuse_width = 6 plan (host data): its six qubits ascending
+/* Block k of a fuse_width = 5 or 6 plan (host data): its six qubits ascending
  * (local index bit b = qubits[b]) and its 64 x 64 unitary, row-major complex
  * (re, im) in u[2 * 64 * 64]; *is_perm = 1 for a VSWAP kept as a permutation
  * (qubits then holds its targets, unused entries -1). */

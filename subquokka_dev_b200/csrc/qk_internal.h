@@ -148,7 +148,9 @@ struct DenseBlock {
     Op perm_op;
     int ngates = 0;
 };
-int build_dense_blocks(const qk_gate *gates, size_t ng, int n, std::vector<DenseBlock> &blocks);
+// width (5 or 6): most qubits a block's gates may touch; blocks are padded to
+// kDenseQubits with idle qubits.
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::vector<DenseBlock> &blocks);
 // Backward sweep of an adjoint gradient: the inverses of gates[ng-1..0] on
 // (psi, lambda), with the gradient of trainable gates (pidx[i] >= 0) taken
 // just before their inverse.

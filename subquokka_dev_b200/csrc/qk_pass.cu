@@ -377,14 +377,15 @@ int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_op
     if (nqubits < 1 || nqubits > 36) return fail(QK_ERR_ARG, "nqubits must be in [1, 36], got %d", nqubits);
     const int dtype = opts ? opts->dtype : QK_C128;
     if (opts && opts->fuse_width) {
-        if (opts->fuse_width != kDenseQubits) return fail(QK_ERR_ARG, "fuse_width must be 0 or %d", kDenseQubits);
+        if (opts->fuse_width != 5 && opts->fuse_width != kDenseQubits)
+            return fail(QK_ERR_ARG, "fuse_width must be 0, 5 or %d", kDenseQubits);
         if (dtype != QK_C64) return fail(QK_ERR_UNSUPPORTED, "tensor-core dense blocks run on complex64 states");
         if (nqubits < 12) return fail(QK_ERR_UNSUPPORTED, "tensor-core dense blocks need at least 12 qubits");
         auto *p = new qk_plan();
         p->dense = true;
         p->hp.n = nqubits;
         p->hp.dtype = dtype;
-        int rc = build_dense_blocks(gates, n, nqubits, p->blocks);
+        int rc = build_dense_blocks(gates, n, nqubits, opts->fuse_width, p->blocks);
         if (rc) {
             delete p;
             return rc;

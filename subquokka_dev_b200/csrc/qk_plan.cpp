@@ -492,8 +492,9 @@ static void block_apply(std::vector<double> &u, const Op &op, const int *loc) {
     }
 }
 
-int build_dense_blocks(const qk_gate *gates, size_t ng, int n, std::vector<DenseBlock> &blocks) {
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::vector<DenseBlock> &blocks) {
     if (n < kDenseQubits) return fail(QK_ERR_ARG, "dense blocks need at least %d qubits", kDenseQubits);
+    if (width < 2 || width > kDenseQubits) return fail(QK_ERR_ARG, "block width must be in [2, %d], got %d", kDenseQubits, width);
     std::vector<Op> ops;
     int rc = lower_all(gates, ng, n, ops);
     if (rc) return rc;
@@ -523,7 +524,7 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, std::vector<Dense
                 int need = 0;
                 for (int k = 0; k < op.nq; ++k)
                     if (std::find(Q.begin(), Q.end(), op.q[k]) == Q.end()) ++need;
-                ok = (int)Q.size() + need <= kDenseQubits;
+                ok = (int)Q.size() + need <= width;
                 if (ok)
                     for (int k = 0; k < op.nq; ++k)
                         if (std::find(Q.begin(), Q.end(), op.q[k]) == Q.end()) Q.push_back(op.q[k]);

@@ -269,7 +269,7 @@ class Plan:
         check(self._lib.qk_plan_apply(sv.h, self.h))
 
     def dense_block(self, k: int):
-        """(qubits, 64 x 64 unitary or None, is_perm) of block k of a fuse_width = 6 plan."""
+        """(qubits, 64 x 64 unitary or None, is_perm) of block k of a fuse_width = 5 or 6 plan."""
         qs = (c_int32 * 6)()
         u = np.zeros(2 * 64 * 64)
         perm = c_int()

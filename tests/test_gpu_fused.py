@@ -125,14 +125,15 @@ def fidelity_err(out, ref):
     return 1 - abs(ov) ** 2 / (np.vdot(ref, ref).real * np.vdot(out, out).real)
 
 
-@pytest.mark.parametrize("n", [12, 14, 17])
-def test_tensor_core_dense_blocks(n):
-    # 6-qubit blocks as 64 x 64 complex contractions on tcgen05 (3 x BF16,
-    # FP32 accumulate): 1 - F <= 1e-6 against the FP64 oracle
+@pytest.mark.parametrize("n,width", [(12, 6), (14, 6), (17, 6), (13, 5), (17, 5)])
+def test_tensor_core_dense_blocks(n, width):
+    # 6-qubit blocks (or 5-qubit blocks padded to 6) as 64 x 64 complex
+    # contractions on tcgen05 (3 x BF16, FP32 accumulate): 1 - F <= 1e-6
+    # against the FP64 oracle
     circ = random_circuit(n, 200, 300 + n)
     init = circuits.random_state(n, 31)
     ref = oracle.apply_circuit(init, n, circ)
-    out = run_plan(n, circ, init, "c64", fuse_width=6)
+    out = run_plan(n, circ, init, "c64", fuse_width=width)
     assert fidelity_err(out, ref) <= 1e-6
     assert np.abs(out - ref).max() <= 5e-5
 

@@ -59,13 +59,27 @@ def apply_block(state, n, qubits, u):
     return np.moveaxis(t.reshape([2] * 6 + [2] * (n - 6)), list(range(6)), axes).reshape(-1)
 
 
+def idle_qubits(u):
+    """Local bits b on which the 64 x 64 unitary u acts as the identity."""
+    idle = []
+    for b in range(6):
+        t = u.reshape([2] * 12)          # axes 0-5: row bits 5..0, axes 6-11: column bits 5..0
+        a_row, a_col = 5 - b, 11 - b
+        blocks = [[t.take(i, a_row).take(j, a_col - 1) for j in range(2)] for i in range(2)]
+        if np.allclose(blocks[0][1], 0, atol=1e-12) and np.allclose(blocks[1][0], 0, atol=1e-12) \
+                and np.allclose(blocks[0][0], blocks[1][1], atol=1e-12):
+            idle.append(b)
+    return idle
+
+
+@pytest.mark.parametrize("width", [5, 6])
 @pytest.mark.parametrize("seed", [1, 2])
-def test_dense_fuser_blocks_reproduce_the_circuit(seed):
+def test_dense_fuser_blocks_reproduce_the_circuit(seed, width):
     import oracle
     from test_gpu_fused import random_circuit
     n = 12
     circ = random_circuit(n, 150, seed)
-    p = Plan(circ, n, "c64", fuse_width=6)
+    p = Plan(circ, n, "c64", fuse_width=width)
     nb = p.stats()[0]
     s = circuits.random_state(n, seed)
     out = s.copy()
@@ -75,8 +89,17 @@ def test_dense_fuser_blocks_reproduce_the_circuit(seed):
             out = oracle.apply_circuit(out, n, Circuit([make_gate("VSWAP", qs)]))
         else:
             assert np.allclose(u.conj().T @ u, np.eye(64), atol=1e-12)
+            assert len(idle_qubits(u)) >= 6 - width     # width 5: one padded, idle qubit
             out = apply_block(out, n, qs, u)
     assert np.abs(out - oracle.apply_circuit(s, n, circ)).max() < 1e-12
+
+
+def test_fuse_width_must_be_5_or_6():
+    c = circuits.random_u3_cz(14, 2, 3)
+    for w in (1, 4, 7):
+        with pytest.raises(sq.QkError):
+            Plan(c, 14, "c64", fuse_width=w)
+    assert Plan(c, 14, "c64", fuse_width=5).stats()[0] > Plan(c, 14, "c64", fuse_width=6).stats()[0]
 
 
 def test_dense_fuser_block_count():
