@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "qk_devplan.h"
+#include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_kernels.cuh"
 
@@ -169,13 +170,7 @@ static int cuda_err(cudaError_t e, const char *what) {
 }
 
 static unsigned red_grid(uint64_t items) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+    const int sms = device_sms();
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + kRedThreads - 1) / kRedThreads, (uint64_t)sms * 8));
 }
 

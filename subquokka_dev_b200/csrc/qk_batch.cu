@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "qk_devplan.h"
+#include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_pass_device.cuh"
 
@@ -367,18 +368,10 @@ static int build_tables(qk_batch *b) {
 
 template <typename C, int R, int NS>
 static int launch_batch_step(const qk_batch::Step &s, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_pass_batch<C, R, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 << 10);
-        if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(k_pass_batch)");
-        attr = true;
-    }
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
+    static std::atomic<uint64_t> smem_done{0};
+    const cudaError_t ea = smem_limit_once(smem_done, (const void *)k_pass_batch<C, R, NS>, 220 << 10);
+    if (ea != cudaSuccess) return cuda_err(ea, "cudaFuncSetAttribute(k_pass_batch)");
+    const int sms = device_sms();
     const unsigned threads = (1u << s.T) / R;
     int mb = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass_batch<C, R, NS>, (int)threads, s.smem);

@@ -38,6 +38,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_pass_device.cuh"
 
@@ -474,15 +475,10 @@ DenseDesc dense_block_desc(const DenseBlock &b, int n) {
 template <int NROWS, bool STATE_N>
 static int launch_dense_tc_n(float2 *state, int n, const DenseDesc &dd, const uint16_t *dW, int *derr,
                              cudaStream_t st) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaError_t e =
-            cudaFuncSetAttribute(k_dense_tc<NROWS, STATE_N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-        if (e != cudaSuccess) return fail(QK_ERR_CUDA, "cudaFuncSetAttribute(k_dense_tc): %s", cudaGetErrorString(e));
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
+    static std::atomic<uint64_t> smem_done{0};
+    const cudaError_t ea = smem_limit_once(smem_done, (const void *)k_dense_tc<NROWS, STATE_N>, (int)kTcSmem);
+    if (ea != cudaSuccess) return fail(QK_ERR_CUDA, "cudaFuncSetAttribute(k_dense_tc): %s", cudaGetErrorString(ea));
+    const int sms = device_sms();
     const uint64_t nsup = 1ull << (n - dd.p.T);
     const unsigned grid = (unsigned)std::min<uint64_t>(nsup, (uint64_t)sms);
     k_dense_tc<NROWS, STATE_N><<<grid, kTcThreads, kTcSmem, st>>>(state, nsup, dd, dW, derr);

@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 
+#include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_kernels.cuh"
 
@@ -71,16 +72,7 @@ static int cuda_fail(cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
-static int num_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    return sms;
-}
+static int num_sms() { return device_sms(); }
 
 static unsigned sweep_blocks(uint64_t items) {
     return (unsigned)std::max<uint64_t>(1, (items + kBlock * kUnroll - 1) / (kBlock * kUnroll));

@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_kernels.cuh"
 #include "qk_devplan.h"
@@ -150,19 +151,15 @@ template <typename C> struct PassArgs {
 
 template <typename C, int R, int NS>
 static int launch_pass_r(const PassArgs<C> &a, int n, const PassDesc &d, cudaStream_t st) {
-    static int sms = 0;
+    static std::atomic<uint64_t> smem_done{0};
     const size_t tile = (sizeof(C) << d.T) * NS;
     const int nbuf = d.perm ? 1 : (2 * tile <= (200u << 10) ? 2 : 1);
     const size_t smem = tile * nbuf + d.nprog * sizeof(TOp) + d.ncoef * sizeof(C) + (NS == 2 ? d.ngrad * sizeof(double) : 0);
     if (smem > (220u << 10)) return fail(QK_ERR_ARG, "pass needs %zu bytes of shared memory", smem);
     cudaError_t e;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaFuncSetAttribute(k_pass<C, R, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 << 10);
-        if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(k_pass)");
-    }
+    e = smem_limit_once(smem_done, (const void *)k_pass<C, R, NS>, 220 << 10);
+    if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(k_pass)");
+    const int sms = device_sms();
     const uint32_t threads = d.perm ? std::max<uint32_t>(1, std::min<uint32_t>(kPassThreads, 1u << d.T))
                                     : (uint32_t)((1u << d.T) / R);
     if (threads > kPassThreads || threads == 0) return fail(QK_ERR_ARG, "pass of %d tile bits needs %u threads", d.T, threads);

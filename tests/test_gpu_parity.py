@@ -226,3 +226,41 @@ def test_out_of_memory_is_an_error_not_a_fault():
     assert e.value.code == -7
     with StateVector(10) as sv:              # the context is still usable
         sv.apply(circuits.qft(10))
+
+
+def test_distinct_handles_on_two_host_threads():
+    # calls on distinct state handles are thread-safe: two host threads, each
+    # with its own state and CUDA stream, run per-gate and fused circuits at
+    # the same time and get the oracle's states
+    import threading
+    import torch
+    from subquokka_dev_b200 import Plan
+    n = 16
+    circs = [circuits.random_u3_cz(n, 6, 70 + k) for k in range(2)]
+    inits = [circuits.random_state(n, 80 + k) for k in range(2)]
+    refs = [oracle.apply_circuit(oracle.apply_circuit(inits[k], n, circs[k]), n, circs[k]) for k in range(2)]
+    out, errs = [None, None], []
+
+    def work(k):
+        try:
+            stream = torch.cuda.Stream()
+            plan = Plan(circs[k], n)
+            with StateVector(n) as sv:
+                sv.set_stream(stream.cuda_stream)
+                for _ in range(5):
+                    sv.upload(inits[k])
+                    sv.apply(circs[k])          # per-gate path
+                    plan.apply(sv)              # fused passes
+                out[k] = sv.download()
+            plan.close()
+        except Exception as e:  # reported below, after both threads end
+            errs.append(e)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for k in range(2):
+        assert np.abs(out[k] - refs[k]).max() <= 1e-12
