@@ -41,8 +41,8 @@ template <typename C> struct BatchEntry {
 
 // One persistent launch over the k-th pass of every circuit.
 template <typename C, int R, int NS>
-__global__ void __launch_bounds__(kPassThreads) k_pass_batch(const BatchEntry<C> *__restrict__ tab, int nent,
-                                                             uint64_t total, uint64_t chunk) {
+__global__ void __launch_bounds__(pass_max_threads<C, R, NS>()) k_pass_batch(const BatchEntry<C> *__restrict__ tab,
+                                                                            int nent, uint64_t total, uint64_t chunk) {
     constexpr int LOG2R = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ PassDesc sd;
@@ -390,16 +390,12 @@ static int launch_step(const qk_batch::Step &s, cudaStream_t st) {
         switch (s.r) {
         case 2: return launch_batch_step<C, 4, 1>(s, st);
         case 3: return launch_batch_step<C, 8, 1>(s, st);
-        case 4:
-            if constexpr (sizeof(C) == sizeof(float2)) return launch_batch_step<C, 16, 1>(s, st);
-            break;
+        case 4: return launch_batch_step<C, 16, 1>(s, st);
         }
     } else {
         switch (s.r) {
         case 2: return launch_batch_step<C, 4, 2>(s, st);
-        case 3:
-            if constexpr (sizeof(C) == sizeof(float2)) return launch_batch_step<C, 8, 2>(s, st);
-            break;
+        case 3: return launch_batch_step<C, 8, 2>(s, st);
         }
     }
     return fail(QK_ERR_ARG, "reg_bits %d unsupported in batched passes", s.r);

@@ -30,7 +30,7 @@ namespace qk {
 // gradient accumulators of the pass live in shared memory and are added to
 // ggrad[gparams[grad0 + i]] once per CTA.
 template <typename C, int R, int NS>
-__global__ void __launch_bounds__(kPassThreads) k_pass(C *__restrict__ s, C *__restrict__ s2, uint64_t ntiles,
+__global__ void __launch_bounds__(pass_max_threads<C, R, NS>()) k_pass(C *__restrict__ s, C *__restrict__ s2, uint64_t ntiles,
                                                        const __grid_constant__ PassDesc d, const TOp *__restrict__ gprog,
                                                        const C *__restrict__ gcoef, const int32_t *__restrict__ gparams,
                                                        double *__restrict__ ggrad, int nbuf) {
@@ -203,8 +203,7 @@ static int launch_pass(C *s, int n, int r, const PassDesc &d, const TOp *ops, co
         case 1: return launch_pass_r<C, 2, 2>(a, n, d, st);
         case 2: return launch_pass_r<C, 4, 2>(a, n, d, st);
         case 3:
-            if constexpr (sizeof(C) == sizeof(float2)) return launch_pass_r<C, 8, 2>(a, n, d, st);
-            break;
+            return launch_pass_r<C, 8, 2>(a, n, d, st);
         }
         return fail(QK_ERR_ARG, "reg_bits %d unsupported for two-state passes", r);
     }
@@ -212,9 +211,7 @@ static int launch_pass(C *s, int n, int r, const PassDesc &d, const TOp *ops, co
     case 1: return launch_pass_r<C, 2, 1>(a, n, d, st);
     case 2: return launch_pass_r<C, 4, 1>(a, n, d, st);
     case 3: return launch_pass_r<C, 8, 1>(a, n, d, st);
-    case 4:
-        if constexpr (sizeof(C) == sizeof(float2)) return launch_pass_r<C, 16, 1>(a, n, d, st);
-        break;
+    case 4: return launch_pass_r<C, 16, 1>(a, n, d, st);
     }
     return fail(QK_ERR_ARG, "reg_bits %d unsupported", r);
 }

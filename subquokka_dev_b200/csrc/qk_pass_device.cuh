@@ -27,6 +27,14 @@ __device__ __forceinline__ uint64_t pass_off(uint32_t j, const PassDesc &d) {
     return g;
 }
 
+// Threads per CTA bound of a pass kernel: 512, or 256 when a thread's
+// register amplitudes take 256 bytes (complex128 with 16 amplitudes, or 8 of
+// each of two states; about 220-240 registers a thread).
+template <typename C, int R, int NS>
+constexpr int pass_max_threads() {
+    return sizeof(C) * R * NS >= 256 ? 256 : kPassThreads;
+}
+
 // Scatter the low bits of v into the set bits of mask, lowest first.
 __device__ __forceinline__ uint32_t deposit_bits(uint32_t v, uint32_t mask) {
     uint32_t r = 0;

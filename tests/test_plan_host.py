@@ -34,7 +34,7 @@ def test_group_plan_one_pass_per_fitting_group():
     assert Plan(c, 12, "c128", groups=True).stats()[0] == 3
 
 
-@pytest.mark.parametrize("dtype,tile,reg", [("c128", 13, 3), ("c128", 12, 4), ("c64", 12, 5), ("c128", 12, 0)])
+@pytest.mark.parametrize("dtype,tile,reg", [("c128", 13, 3), ("c128", 13, 4), ("c128", 12, 5), ("c64", 12, 5), ("c128", 12, 0)])
 def test_bad_options_rejected(dtype, tile, reg):
     c = circuits.qft(14)
     if reg == 0:
