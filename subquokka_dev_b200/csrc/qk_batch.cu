@@ -693,9 +693,9 @@ int qk_batch_create(int ncirc, const int32_t *nqubits, const qk_gate *gates, con
         // try tile shapes on the real batch, keep the fastest forward and adjoint
         struct Cand { int T, r; };
         const std::vector<Cand> fc = b->dtype == QK_C64 ? std::vector<Cand>{{12, 3}, {12, 4}, {13, 4}}
-                                                        : std::vector<Cand>{{12, 3}, {11, 3}};
+                                                        : std::vector<Cand>{{11, 4}, {12, 3}, {11, 3}};
         const std::vector<Cand> bc = b->dtype == QK_C64 ? std::vector<Cand>{{11, 3}, {12, 3}}
-                                                        : std::vector<Cand>{{11, 2}, {10, 2}};
+                                                        : std::vector<Cand>{{11, 3}, {11, 2}, {10, 2}};
         float best = 1e30f;
         PlanOptions bf = b->fo, bb = b->bo;
         for (const auto &f : fc)
