@@ -189,6 +189,17 @@ int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes,
 int qk_apply_gates_dev(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n,
                        void *cuda_stream);
 
+/* The per-gate path (qk_apply_gates' launches) captured once as a CUDA
+ * graph bound to sv's state and replayed on sv's stream: the same kernels and
+ * results, one launch for the whole gate list.  For small states, where a
+ * gate's kernel runs for about as long as the host takes to launch it.  The
+ * graph must not outlive sv.  No reference counterpart (MEM_Runner::run
+ * loops over the gates, src/MEM_Runner.cpp:101-134). */
+typedef struct qk_graph qk_graph;
+int qk_graph_create(qk_sv *sv, const qk_gate *gates, size_t ngates, qk_graph **out);
+int qk_graph_launch(qk_graph *g);
+void qk_graph_destroy(qk_graph *g);
+
 /* Per-gate path with a CUDA event pair around every gate's kernel on the
  * state's stream; gate_ms[i] receives gate i's device time in milliseconds.
  * Synchronises the stream before returning.  Used for per-kernel rooflines. */

@@ -102,6 +102,9 @@ PROTOTYPES = {
     "qk_sv_synchronize": (c_int, [c_void_p]),
     "qk_sv_release_workspace": (c_int, [c_void_p]),
     "qk_apply_gates": (c_int, [c_void_p, POINTER(QkGate), c_size_t]),
+    "qk_graph_create": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_void_p)]),
+    "qk_graph_launch": (c_int, [c_void_p]),
+    "qk_graph_destroy": (None, [c_void_p]),
     "qk_apply_groups": (c_int, [c_void_p, POINTER(QkGate), POINTER(c_int32), c_size_t]),
     "qk_apply_gates_dev": (c_int, [c_void_p, c_int, c_int, POINTER(QkGate), c_size_t, c_void_p]),
     "qk_apply_gates_timed": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(ctypes.c_float)]),

@@ -291,6 +291,71 @@ int qk_apply_gates(qk_sv *sv, const qk_gate *gates, size_t n) {
     return qk_apply_gates_dev(sv->d, sv->n, sv->dtype, gates, n, sv->stream);
 }
 
+// ---- the per-gate path as a CUDA graph -------------------------------------
+
+struct qk_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    qk_sv *sv = nullptr;
+};
+
+int qk_graph_create(qk_sv *sv, const qk_gate *gates, size_t n, qk_graph **out) {
+    if (!sv || !out || (!gates && n)) return fail(QK_ERR_ARG, "null argument");
+    std::vector<Op> ops(n);
+    for (size_t i = 0; i < n; ++i) {
+        int rc = lower_gate(gates[i], ops[i]);
+        if (rc) return rc;
+        for (int k = 0; k < ops[i].nq; ++k)
+            if (ops[i].q[k] < 0 || ops[i].q[k] >= sv->n)
+                return fail(QK_ERR_QUBIT, "gate %zu: qubit %d outside a %d-qubit state", i, ops[i].q[k], sv->n);
+    }
+    // capture the same launches qk_apply_gates makes, on a private stream
+    // (thread-local mode: other threads' CUDA calls are unaffected)
+    cudaStream_t cs = nullptr;
+    QK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return cuda_fail(e, "cudaStreamBeginCapture");
+    }
+    int rc = QK_OK;
+    for (size_t i = 0; i < n && !rc; ++i) rc = launch_gate_op(sv->d, sv->n, sv->dtype, ops[i], cs);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    auto *h = new qk_graph();
+    h->graph = g;
+    h->exec = ex;
+    h->sv = sv;
+    *out = h;
+    clear_error();
+    return QK_OK;
+}
+
+int qk_graph_launch(qk_graph *g) {
+    if (!g) return fail(QK_ERR_ARG, "null graph");
+    QK_CUDA(cudaGraphLaunch(g->exec, g->sv->stream));
+    clear_error();
+    return QK_OK;
+}
+
+void qk_graph_destroy(qk_graph *g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
 int qk_apply_gates_timed(qk_sv *sv, const qk_gate *gates, size_t n, float *gate_ms) {
     if (!sv || !gate_ms || (!gates && n)) return fail(QK_ERR_ARG, "null argument");
     std::vector<cudaEvent_t> ev(n + 1);

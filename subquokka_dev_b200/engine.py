@@ -233,9 +233,45 @@ class StateVector:
         """Per-gate path (MEM_Runner::run(vector<Gate*>&))."""
         check(self._lib.qk_apply_gates(self.h, circuit.gates, circuit.ngates))
 
+    def capture(self, circuit: Circuit) -> "GateGraph":
+        """The per-gate path for `circuit` captured as a CUDA graph on this
+        state: `graph.launch()` applies the circuit again with one launch."""
+        return GateGraph(self, circuit)
+
     def apply_groups(self, circuit: Circuit) -> None:
         """Subcircuit path (MEM_Runner::run(vector<vector<Gate*>>&))."""
         check(self._lib.qk_apply_groups(self.h, circuit.gates, circuit.group_sizes, circuit.ngroups))
+
+
+class GateGraph:
+    """qk_graph_*: the per-gate kernels of a circuit as one CUDA graph bound
+    to a state (close it before the state)."""
+
+    def __init__(self, sv: "StateVector", circuit: Circuit):
+        self._lib = _lib.load()
+        self.sv = sv
+        self.h = c_void_p()
+        check(self._lib.qk_graph_create(sv.h, circuit.gates, circuit.ngates, byref(self.h)))
+
+    def launch(self) -> None:
+        check(self._lib.qk_graph_launch(self.h))
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.qk_graph_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class Plan:

@@ -264,3 +264,34 @@ def test_distinct_handles_on_two_host_threads():
     assert not errs, errs
     for k in range(2):
         assert np.abs(out[k] - refs[k]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_gate_graph_replays_the_per_gate_path(dtype):
+    # the per-gate kernels captured as one CUDA graph give the per-gate path's
+    # amplitudes bit for bit, launch after launch (SWAP, VSWAP_1_1 and
+    # VSWAP_2_2 permutations included)
+    n = 13
+    gates = list(circuits.qft(n).gate_list())
+    gates += [make_gate("VSWAP", [0, 1, 9, 11]), make_gate("VSWAP", [2, 12]), make_gate("SWAP", [3, 7])]
+    gates += list(circuits.random_u3_cz(n, 2, 5).gate_list())
+    circ = Circuit(gates)
+    init = circuits.random_state(n, 6)
+    with StateVector(n, dtype) as a, StateVector(n, dtype) as b:
+        a.upload(init)
+        b.upload(init)
+        with b.capture(circ) as g:
+            for _ in range(3):
+                a.apply(circ)
+                g.launch()
+                assert np.array_equal(a.download(), b.download())
+    ref = init
+    for _ in range(3):
+        ref = oracle.apply_circuit(ref, n, circ)
+    tol = 1e-12 if dtype == "c128" else 2e-5
+    with StateVector(n, dtype) as c:
+        c.upload(init)
+        with c.capture(circ) as g:
+            for _ in range(3):
+                g.launch()
+        assert np.abs(c.download() - ref).max() <= tol
