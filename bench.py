@@ -249,7 +249,8 @@ def compare_states(a, b):
         ov += complex(torch.vdot(xs, ys))
         nx += float(torch.vdot(xs, xs).real)
         ny += float(torch.vdot(ys, ys).real)
-    return dmax, 1.0 - abs(ov) ** 2 / (nx * ny)
+    # 1 - F below the rounding of the sums (|values| ~1e-16) reads as 0
+    return dmax, max(0.0, 1.0 - abs(ov) ** 2 / (nx * ny))
 
 
 def fused_variants(args, circ, exact, plain_ms, alg):
