@@ -96,6 +96,7 @@ struct TOp {
     uint32_t coef;
 };
 static_assert(sizeof(TOp) == 16, "TOp must stay 16 bytes");
+constexpr uint8_t kNoSlot = 0xFF;   // TOp.bits[k] of a condition qubit held in no register slot
 
 struct PassDesc {
     int32_t T;                    // tile bits

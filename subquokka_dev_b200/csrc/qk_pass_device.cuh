@@ -207,6 +207,22 @@ __device__ __forceinline__ uint32_t bit_set(uint8_t code, uint32_t none, uint64_
     return (tb & m) ? 0xFFFFFFFFu : 0u;
 }
 
+// The same two lookups with the register slot supplied by the planner
+// (kNoSlot: the qubit is a thread bit, an outer bit, or none).
+__device__ __forceinline__ uint32_t bit_set_at(uint8_t code, uint8_t slot, uint32_t none, uint64_t base, uint32_t tb) {
+    if (slot != kNoSlot) return slot_pattern(slot);
+    if (code == kNoQubit) return none ? 0xFFFFFFFFu : 0u;
+    if (code & kOuterFlag) return ((base >> (code & 0x7F)) & 1) ? 0xFFFFFFFFu : 0u;
+    return (tb >> code) & 1 ? 0xFFFFFFFFu : 0u;
+}
+__device__ __forceinline__ int code_slot_at(uint8_t code, uint8_t slot, uint64_t base, uint32_t tb, uint32_t *bit) {
+    *bit = 0;
+    if (slot != kNoSlot) return slot;
+    if (code == kNoQubit) return -1;
+    *bit = (code & kOuterFlag) ? (uint32_t)(base >> (code & 0x7F)) & 1u : (tb >> code) & 1u;
+    return -1;
+}
+
 // Register slot holding a diagonal-op qubit code, or -1 with *bit set to the
 // qubit's value, which is then the same for every register element.
 template <int LOG2R>
@@ -359,7 +375,7 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             // the same for all of them
             const C d0 = coef[op.coef], d1 = coef[op.coef + 1], d2 = coef[op.coef + 2], d3 = coef[op.coef + 3];
             uint32_t ba, bb;
-            const int sa = code_slot<LOG2R>(op.a, base, tb, bm, &ba), sb = code_slot<LOG2R>(op.b, base, tb, bm, &bb);
+            const int sa = code_slot_at(op.a, op.bits[0], base, tb, &ba), sb = code_slot_at(op.b, op.bits[1], base, tb, &bb);
             if (sa >= 0 && sb >= 0) {
                 switch (sa * 8 + sb) {
 #define QK_D2(A, B)                                                  \
@@ -395,7 +411,7 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             break;
         }
         case TOP_CX: {
-            const uint32_t M = bit_set<LOG2R>(op.b, 1, base, tb, bm);
+            const uint32_t M = bit_set_at(op.b, op.bits[1], 1, base, tb);
             switch (op.a) {
 #define QK_CX(S)                                   \
     case S:                                        \
@@ -409,7 +425,7 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
         }
         case TOP_PHASE: {
             const C ph = coef[op.coef];
-            const uint32_t M = bit_set<LOG2R>(op.a, 1, base, tb, bm) & bit_set<LOG2R>(op.b, 1, base, tb, bm);
+            const uint32_t M = bit_set_at(op.a, op.bits[0], 1, base, tb) & bit_set_at(op.b, op.bits[1], 1, base, tb);
             if (!(M & ((R >= 32) ? 0xFFFFFFFFu : ((1u << R) - 1)))) break;
 #pragma unroll
             for (int kk = 0; kk < R; ++kk)

@@ -265,6 +265,18 @@ struct PassBuilder {
         default:
             break;  // OP_PERM never reaches a compute pass
         }
+        // condition qubits of DIAG / PHASE (a, b) and CX (b): their register
+        // slot in bits[0] / bits[1] (kNoSlot when not register-resident), so
+        // that the kernel need not search the current mapping
+        if (t.kind == TOP_DIAG || t.kind == TOP_PHASE || t.kind == TOP_CX) {
+            auto slot_of = [&](uint8_t c) -> uint8_t {
+                if (c == kNoQubit || (c & kOuterFlag)) return kNoSlot;
+                const auto it = std::find(Q.begin(), Q.end(), (int)c);
+                return it == Q.end() ? kNoSlot : (uint8_t)(it - Q.begin());
+            };
+            t.bits[0] = t.kind == TOP_CX ? kNoSlot : slot_of(t.a);
+            t.bits[1] = slot_of(t.b);
+        }
         plan.ops.push_back(t);
     }
 
