@@ -202,7 +202,8 @@ def test_cli_text_dump_format(tmp_path):
     assert len(vals) == 16 and vals[0] == "%.11f" % (0.70710678118 ** 3) and vals[1] == "0.00000000000"
 
 
-@pytest.mark.parametrize("precision,fuse_width,tol", [("c128", 1, 1e-12), ("c64", 1, 2e-6), ("c64", 6, 5e-5)])
+@pytest.mark.parametrize("precision,fuse_width,tol", [("c128", 1, 1e-12), ("c64", 1, 2e-6), ("c64", 5, 5e-5),
+                                                     ("c64", 6, 5e-5)])
 def test_cli_fused_forms(tmp_path, precision, fuse_width, tol):
     n = 14
     ini = tmp_path / "x.ini"
