@@ -271,9 +271,9 @@ __device__ __forceinline__ uint32_t reg_sidx(int kk, uint32_t stb, const uint32_
 
 // Im <lambda|G|psi> over this thread's register pairs of slot S (G = X, Y, Z
 // by gen 1, 2, 3), summed in the state's precision (a thread holds at most
-// 16 pairs) and returned as a double for the cross-thread reduction.
+// 16 pairs).
 template <int S, typename C, int R>
-__device__ __forceinline__ double reg_grad(const C (&v)[R], const C (&w)[R], int gen) {
+__device__ __forceinline__ auto reg_grad(const C (&v)[R], const C (&w)[R], int gen) {
     using T = decltype(v[0].x);
     T s = 0;
     if constexpr ((1 << S) < R) {
@@ -293,7 +293,7 @@ __device__ __forceinline__ double reg_grad(const C (&v)[R], const C (&w)[R], int
                 if (!(k & (1 << S))) s += im(w[k], v[k]) - im(w[k | (1 << S)], v[k | (1 << S)]);
         }
     }
-    return (double)s;
+    return s;
 }
 
 // Run a pass program on one tile (NS = 1) or on the matching tiles of two
@@ -437,7 +437,9 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
         }
         case TOP_GRAD: {
             if constexpr (NS == 2) {
-                double g = 0;
+                // summed over the warp in the state's precision, added to
+                // the CTA's double accumulator once per warp
+                decltype(v[0].x) g = 0;
                 switch (op.a) {
                 case 0: g = reg_grad<0>(v, w, op.b); break;
                 case 1: g = reg_grad<1>(v, w, op.b); break;
@@ -447,7 +449,7 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
                 }
 #pragma unroll
                 for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
-                if ((tid & 31) == 0) atomicAdd(gsm + op.coef, g);
+                if ((tid & 31) == 0) atomicAdd(gsm + op.coef, (double)g);
             }
             break;
         }
