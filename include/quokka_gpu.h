@@ -145,6 +145,21 @@ void qk_circuit_destroy(qk_circuit *c);
  * permutation matrices of dimension 2^(2k). */
 int qk_gate_matrix(const qk_gate *g, double *out, int *dim);
 
+/* Group a flat gate list into a subcircuit file for the reference's
+ * subcircuit runner: the job of subcircuitFinder (subcircuitFinder/finder.cpp:
+ * 771-877), for every gate of the MEM grammar and any chunk size.  Every
+ * compute group acts on bit positions below chunk_qbit only; single-gate
+ * groups `VSWAP_1_1 a c` / `VSWAP_2_2 a b c d` (a < b < chunk_qbit <= c < d)
+ * move other qubits into the chunk; at the end the state is back in the
+ * input's layout, so the grouped file computes the same state as the flat
+ * one.  VSWAP gates of the input are absorbed as renamings.  *out is a new
+ * circuit (free with qk_circuit_destroy). */
+int qk_circuit_chunk_groups(const qk_gate *gates, size_t n, int nqubits, int chunk_qbit, qk_circuit **out);
+/* Write a circuit in the circuit.txt grammar: one gate per line
+ * (is_subcircuit = 0) or group-count lines each followed by its gates
+ * (is_subcircuit = 1); numbers with 17 significant digits. */
+int qk_circuit_write(const qk_circuit *c, int is_subcircuit, const char *path);
+
 /* ---- state vectors ----------------------------------------------------- */
 
 /* Allocate a 2^nqubits state on the current CUDA device and set it to

@@ -92,6 +92,8 @@ PROTOTYPES = {
     "qk_circuit_group_sizes": (POINTER(c_int32), [c_void_p]),
     "qk_circuit_destroy": (None, [c_void_p]),
     "qk_gate_matrix": (c_int, [POINTER(QkGate), POINTER(c_double), POINTER(c_int)]),
+    "qk_circuit_chunk_groups": (c_int, [POINTER(QkGate), c_size_t, c_int, c_int, POINTER(c_void_p)]),
+    "qk_circuit_write": (c_int, [c_void_p, c_int, c_char_p]),
     "qk_sv_create": (c_int, [c_int, c_int, POINTER(c_void_p)]),
     "qk_sv_destroy": (None, [c_void_p]),
     "qk_sv_reset": (c_int, [c_void_p]),

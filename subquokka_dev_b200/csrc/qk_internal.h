@@ -20,7 +20,7 @@ enum OpKind : int32_t {
     OP_DENSE2 = 3,  // 4x4 matrix on (q[0], q[1]), index bit0=q[0] (U2)
     OP_PHASE2 = 4,  // amplitudes with bits q[0], q[1] set *= m[0] (CP)
     OP_DIAG2 = 5,   // *= m[b0 + 2 b1]                             (RZZ)
-    OP_SWAP2 = 6,   // exchange |01> and |10> of (q[0], q[1])      (SWAP, VSWAP_1_1)
+    OP_SWAP2 = 6,   // exchange |01> and |10> of (q[0], q[1])      (SWAP, VSWAP_1_1: aux = 1)
     OP_PERM = 7,    // swap bit q[i] with bit q[k+i], i < k = nq/2 (VSWAP_k_k)
     OP_GRAD = 8,    // adjoint sweep: grad[aux] += Im <lambda|G|psi>, G on q[0] = X/Y/Z by m[0] = 1/2/3
     OP_CX = 9,      // flip bit q[1 - aux] where bit q[aux] is set (a U2 that is exactly a CNOT)
@@ -30,7 +30,7 @@ struct Op {
     int32_t kind;
     int32_t nq;
     int32_t q[QK_MAX_TARGETS];
-    int32_t aux;   // OP_GRAD: parameter index
+    int32_t aux;   // OP_GRAD: parameter index; OP_CX: control index; OP_SWAP2 / OP_PERM: 1 from a VSWAP
     double m[32];  // complex coefficients, (re, im) interleaved
 };
 
@@ -131,8 +131,10 @@ struct PlanOptions {
 
 // Build a fused plan for a flat gate list (greedy tile-bit choice).
 int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, HostPlan &plan);
-// Build one pass per group (the subcircuit path): every group becomes a pass
-// over the union of its qubits; VSWAP groups become permutation passes.
+// One permutation pass (an OP_PERM of 1 to 6 bit pairs), with no program.
+int build_perm_plan(const Op &op, int n, const PlanOptions &o, HostPlan &plan);
+// Plan of a subcircuit file (the subcircuit path): the gates of all groups
+// as one gate list, VSWAPs as renamings of the qubits after them.
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
                      HostPlan &plan);
 PlanOptions default_plan_options(int dtype, int n);

@@ -237,6 +237,7 @@ int lower_gate(const qk_gate &g, Op &op) {
         // src/circuit.cpp:3457-3556, checked against SWAP(q0,q2) SWAP(q1,q3) by
         // src/correctness/gate_check_MEM.py:314-348).
         op.kind = g.nq == 2 ? OP_SWAP2 : OP_PERM;
+        op.aux = 1;   // a VSWAP: planners may rename qubits instead
         return QK_OK;
     default:
         return fail(QK_ERR_PARSE, "unknown gate kind %d", g.kind);

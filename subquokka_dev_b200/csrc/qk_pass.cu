@@ -195,6 +195,9 @@ static int launch_pass(C *s, int n, int r, const PassDesc &d, const TOp *ops, co
         }
         return QK_OK;
     }
+    // a compute pass reads its program and coefficients from device memory
+    if ((d.nprog && !ops) || (d.ncoef && !coef))
+        return fail(QK_ERR_ARG, "compute pass without its program in device memory");
     PassArgs<C> a{s, s2, ops, coef, gparams, ggrad};
     // register-resident amplitudes per thread: up to 8 complex128 or 16
     // complex64 per state (more would spill)
@@ -349,15 +352,9 @@ int apply_group_plan(qk_sv *sv, const qk_gate *gates, const int32_t *sizes, size
 
 int apply_perm_gate(void *state, int n, int dtype, const Op &op, cudaStream_t st) {
     HostPlan hp;
-    qk_gate g;
-    std::memset(&g, 0, sizeof g);
-    g.kind = QK_GATE_VSWAP;
-    g.nq = op.nq;
-    for (int i = 0; i < op.nq; ++i) g.q[i] = op.q[i];
-    PlanOptions o = default_plan_options(dtype, n);
-    int rc = build_plan(&g, 1, n, o, hp);
+    int rc = build_perm_plan(op, n, default_plan_options(dtype, n), hp);
     if (rc) return rc;
-    DevPlan none;
+    DevPlan none;   // permutation passes run no program
     return run_plan(state, dtype, hp, none, st);
 }
 

@@ -52,6 +52,11 @@ namespace {
 
 int low_bits(int dtype) { return dtype == QK_C128 ? 3 : 4; }  // 128-byte runs
 
+// Most tile bits of a permutation pass (qk_pass.cu stages such a tile in
+// shared memory in one buffer).
+int perm_tile_bits(int dtype) { return dtype == QK_C128 ? 13 : 14; }
+constexpr int kPermMinTileBits = 10;
+
 void push_c(HostPlan &p, double re, double im) {
     p.coef.push_back(re);
     p.coef.push_back(im);
@@ -292,7 +297,11 @@ struct PassBuilder {
             if (!in[q]) { in[q] = 1; ++cnt; }
         d.perm = 1;
         d.nperm = k;
-        if (cnt > (plan.dtype == QK_C128 ? 13 : 14)) {
+        // a few more low bits than the swapped ones need: longer contiguous
+        // runs per tile row (identity on those bits)
+        for (int q = 0; q < n && cnt < kPermMinTileBits && cnt <= perm_tile_bits(plan.dtype); ++q)
+            if (!in[q]) { in[q] = 1; ++cnt; }
+        if (cnt > perm_tile_bits(plan.dtype)) {
             // too many qubits for one tile: flat in-place permutation sweep
             d.perm = 2;
             for (int i = 0; i < k; ++i) { d.perm_a[i] = op.q[i]; d.perm_b[i] = op.q[k + i]; }
@@ -377,6 +386,92 @@ int lower_all(const qk_gate *gates, size_t ng, int n, std::vector<Op> &ops) {
     return QK_OK;
 }
 
+// VSWAP_k_k as a relabelling of qubits.  The reference moves amplitudes for
+// every VSWAP (src/MEM_Runner.cpp:146-167).  Here a VSWAP (and, with swaps
+// set, a SWAP gate too) only swaps entries of bit_of (bit position of the
+// circuit -> bit of the stored state), and the ops after it are renamed
+// through that map.  At the end the stored
+// state is brought into the circuit's layout by at most two rounds of
+// disjoint bit swaps: any permutation is the product of two involutions.
+// The content of stored bit x_i moves to x_{i+1} around each cycle
+// x_0 -> x_1 -> ... -> x_{m-1}; that is the reflection x_i <-> x_{1-i}
+// applied after the reflection x_i <-> x_{-i} (indices mod m).  Each round
+// becomes OP_PERM ops of at most max_pairs pairs whose bits, with the low L
+// state bits, fit max_bits tile bits, so that they run as tile passes.
+bool renamable(const Op &op, bool swaps) {
+    return op.kind == OP_PERM || (op.kind == OP_SWAP2 && (swaps || op.aux == 1));
+}
+
+void relabel_perms(std::vector<Op> &ops, int n, int L, int max_bits, int max_pairs, bool swaps) {
+    bool any = false;
+    for (const Op &op : ops) any = any || renamable(op, swaps);
+    if (!any) return;
+    std::vector<int> bit_of(n);
+    for (int p = 0; p < n; ++p) bit_of[p] = p;
+    std::vector<Op> out;
+    out.reserve(ops.size() + 4);
+    for (const Op &op : ops) {
+        if (renamable(op, swaps)) {
+            const int k = op.nq / 2;
+            for (int i = 0; i < k; ++i) std::swap(bit_of[op.q[i]], bit_of[op.q[k + i]]);
+            continue;
+        }
+        Op r = op;
+        for (int j = 0; j < r.nq; ++j) r.q[j] = bit_of[r.q[j]];
+        out.push_back(r);
+    }
+    std::vector<int> to(n);   // content of stored bit x moves to bit to[x]
+    for (int p = 0; p < n; ++p) to[bit_of[p]] = p;
+    std::vector<std::pair<int, int>> rounds[2];
+    std::vector<char> seen(n, 0);
+    for (int s = 0; s < n; ++s) {
+        if (seen[s] || to[s] == s) continue;
+        std::vector<int> x;
+        for (int c = s; !seen[c]; c = to[c]) {
+            seen[c] = 1;
+            x.push_back(c);
+        }
+        const int m = (int)x.size();
+        for (int i = 1; i < m - i; ++i) rounds[0].push_back({x[i], x[m - i]});
+        for (int j = 0; j < m; ++j) {
+            const int pj = (m + 1 - j) % m;
+            if (j < pj) rounds[1].push_back({x[j], x[pj]});
+        }
+    }
+    for (auto &pairs : rounds) {
+        std::vector<char> used(pairs.size(), 0);
+        size_t left = pairs.size();
+        while (left) {
+            std::vector<char> bits(n, 0);
+            int nbits = 0;
+            for (int q = 0; q < std::min(n, L); ++q) bits[q] = 1, ++nbits;
+            Op op;
+            std::memset(&op, 0, sizeof op);
+            op.kind = OP_PERM;
+            op.aux = 1;
+            std::vector<std::pair<int, int>> take;
+            for (size_t i = 0; i < pairs.size() && (int)take.size() < max_pairs; ++i) {
+                if (used[i]) continue;
+                const int add = !bits[pairs[i].first] + !bits[pairs[i].second];
+                if (!take.empty() && nbits + add > max_bits) continue;
+                bits[pairs[i].first] = bits[pairs[i].second] = 1;
+                nbits += add;
+                take.push_back(pairs[i]);
+                used[i] = 1;
+                --left;
+            }
+            const int k = (int)take.size();
+            op.nq = 2 * k;
+            for (int i = 0; i < k; ++i) {
+                op.q[i] = take[i].first;
+                op.q[k + i] = take[i].second;
+            }
+            out.push_back(op);
+        }
+    }
+    ops.swap(out);
+}
+
 // Leading state bits always in the tile; two tile bits stay free for the
 // qubits of any single gate, so every pass takes at least one gate.
 int pass_low_bits(const PlanOptions &o, int n) {
@@ -407,16 +502,48 @@ int check_options(const PlanOptions &o, int n) {
 int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, HostPlan &plan) {
     int rc = check_options(o, n);
     if (rc) return rc;
-    std::vector<Op> ops;
-    rc = lower_all(gates, ng, n, ops);
+    std::vector<Op> lowered;
+    rc = lower_all(gates, ng, n, lowered);
     if (rc) return rc;
+    // VSWAPs are always renamings.  SWAP gates are too when that gives fewer
+    // passes: their renaming removes them from the compute passes but can
+    // leave a longer permutation to restore at the end.
+    bool swaps = false;
+    for (const Op &op : lowered) swaps = swaps || (op.kind == OP_SWAP2 && op.aux != 1);
+    for (int variant = 0; variant < (swaps ? 2 : 1); ++variant) {
+        std::vector<Op> ops = lowered;
+        relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant == 1);
+        HostPlan hp;
+        hp.n = n;
+        hp.dtype = o.dtype;
+        hp.T = o.tile_bits;
+        hp.r = o.reg_bits;
+        PassBuilder b{ops, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), hp};
+        rc = b.greedy(0, ops.size());
+        if (rc) return rc;
+        if (variant == 0 || hp.passes.size() < plan.passes.size() ||
+            (hp.passes.size() == plan.passes.size() && hp.ops.size() < plan.ops.size()))
+            plan = std::move(hp);
+    }
+    return QK_OK;
+}
+
+int build_perm_plan(const Op &op, int n, const PlanOptions &o, HostPlan &plan) {
+    if (op.kind != OP_PERM || op.nq < 2 || op.nq % 2 || op.nq > 12)
+        return fail(QK_ERR_ARG, "not a permutation of 1 to 6 bit pairs");
+    for (int i = 0; i < op.nq; ++i)
+        if (op.q[i] < 0 || op.q[i] >= n) return fail(QK_ERR_QUBIT, "qubit %d outside a %d-qubit state", op.q[i], n);
+    int rc = check_options(o, n);
+    if (rc) return rc;
+    std::vector<Op> ops{op};
     plan = HostPlan();
     plan.n = n;
     plan.dtype = o.dtype;
     plan.T = o.tile_bits;
     plan.r = o.reg_bits;
     PassBuilder b{ops, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), plan};
-    return b.greedy(0, ops.size());
+    b.perm_pass(op);
+    return QK_OK;
 }
 
 int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int n, const PlanOptions &o,
@@ -516,6 +643,9 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::v
     std::vector<Op> ops;
     int rc = lower_all(gates, ng, n, ops);
     if (rc) return rc;
+    // at most three pairs per restoring permutation: a permutation block
+    // lists its targets in kDenseQubits entries
+    relabel_perms(ops, n, low_bits(QK_C64), perm_tile_bits(QK_C64), kDenseQubits / 2, false);
     blocks.clear();
     std::vector<size_t> pending(ops.size());
     for (size_t i = 0; i < ops.size(); ++i) pending[i] = i;
@@ -620,54 +750,15 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::v
 
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
                      HostPlan &plan) {
-    int rc = check_options(o, n);
-    if (rc) return rc;
     size_t ng = 0;
     for (size_t g = 0; g < ngroups; ++g) {
         if (sizes[g] < 0) return fail(QK_ERR_ARG, "group %zu has negative size", g);
         ng += (size_t)sizes[g];
     }
-    std::vector<Op> ops;
-    rc = lower_all(gates, ng, n, ops);
-    if (rc) return rc;
-    plan = HostPlan();
-    plan.n = n;
-    plan.dtype = o.dtype;
-    plan.T = o.tile_bits;
-    plan.r = o.reg_bits;
-    const int L = pass_low_bits(o, n);
-    PassBuilder b{ops, n, o.tile_bits, o.reg_bits, L, plan};
-    size_t g0 = 0;
-    for (size_t g = 0; g < ngroups; ++g) {
-        const size_t cnt = (size_t)sizes[g];
-        if (!cnt) continue;
-        // one pass per group when the union of its non-diagonal qubits fits a
-        // tile (the reference's requirement that a group sit in one chunk);
-        // otherwise the group is split greedily
-        std::vector<int> B;
-        for (int q = 0; q < std::min(n, L); ++q) B.push_back(q);
-        bool fits = true;
-        size_t used = 0;
-        for (size_t i = g0; i < g0 + cnt && fits; ++i) {
-            if (ops[i].kind == OP_PERM) { fits = false; break; }
-            used += op_cost(ops[i], o.dtype);
-            if (used > program_budget(o.dtype, o.tile_bits, 1)) { fits = false; break; }
-            for (int k = op_reg_first(ops[i]); k < op_reg_first(ops[i]) + op_reg_count(ops[i]); ++k)
-                if (std::find(B.begin(), B.end(), ops[i].q[k]) == B.end()) B.push_back(ops[i].q[k]);
-            fits = (int)B.size() <= o.tile_bits;
-        }
-        if (fits) {
-            b.fill(B);
-            std::vector<int> idx;
-            for (size_t i = g0; i < g0 + cnt; ++i) idx.push_back((int)i);
-            rc = b.compile(idx, B);
-        } else {
-            rc = b.greedy(g0, g0 + cnt);
-        }
-        if (rc) return rc;
-        g0 += cnt;
-    }
-    return QK_OK;
+    // The groups bound nothing here: a tile can hold any qubits, and VSWAP
+    // groups become renamings, so the gates of all groups are planned as one
+    // gate list.
+    return build_plan(gates, ng, n, o, plan);
 }
 
 }  // namespace qk

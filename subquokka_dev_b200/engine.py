@@ -112,6 +112,17 @@ class Circuit:
         return "\n".join(lines) + "\n"
 
 
+def chunk_groups(circuit: Circuit, n: int, chunk_qbit: int = 12) -> Circuit:
+    """The subcircuit file of a flat circuit for the reference's subcircuit
+    runner (the output subcircuitFinder makes, subcircuitFinder/finder.cpp:
+    771-877): compute groups on bit positions below chunk_qbit, VSWAP_1_1 /
+    VSWAP_2_2 groups between them, the state back in the input's layout at
+    the end.  ``.to_text(True)`` is the file's text."""
+    h = c_void_p()
+    check(_lib.load().qk_circuit_chunk_groups(circuit.gates, circuit.ngates, int(n), int(chunk_qbit), byref(h)))
+    return Circuit._from_handle(h)
+
+
 def parse_line(line: str, total_qbit: int) -> QkGate:
     g = QkGate()
     check(_lib.load().qk_gate_parse_line(line.encode(), int(total_qbit), byref(g)))

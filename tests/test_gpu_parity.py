@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
-from subquokka_dev_b200 import Circuit, StateVector, apply_gates_dev, circuits, make_gate
+from subquokka_dev_b200 import Circuit, StateVector, apply_gates_dev, chunk_groups, circuits, make_gate
 
 import golden_util as gu
 
@@ -129,6 +129,21 @@ def test_random_circuit_family_matches_oracle():
     ref = oracle.apply_circuit(gu.initial_state({"n": n, "sampled": False, "init": np.zeros(0)}), n, circ)
     assert np.abs(run_gpu(n, circ, None) - ref).max() <= TOL_C128
     assert np.abs(run_gpu(n, circ, None, groups=True) - ref).max() <= TOL_C128
+
+
+@pytest.mark.parametrize("dtype,tol", [("c128", TOL_C128), ("c64", TOL_C64)])
+@pytest.mark.parametrize("name", ["qft", "u3cz"])
+def test_chunk_grouped_file_through_group_path(name, dtype, tol):
+    # a subcircuit file from chunk_groups (12-qubit chunks, VSWAP_2_2 /
+    # VSWAP_1_1 groups between the compute groups) through the group path:
+    # the VSWAPs become renamings and the result is the flat circuit's state
+    n = 22
+    circ = circuits.qft(n) if name == "qft" else circuits.random_u3_cz(n, 8, 4)
+    sub = chunk_groups(circ, n, 12)
+    assert sum(1 for i in range(sub.ngates) if sub.gates[i].kind == 14) >= 4
+    init = circuits.random_state(n, 12)
+    ref = oracle.apply_circuit(init, n, circ)
+    assert np.abs(run_gpu(n, sub, init, dtype, groups=True) - ref).max() <= tol
 
 
 def inverse(circ):
