@@ -254,15 +254,20 @@ def compare_states(a, b):
 
 
 def fused_variants(args, circ, exact, plain_ms, alg):
-    """The same circuit through fused passes, complex128 and complex64; each is
-    compared with the exact per-gate complex128 state left in `exact`."""
+    """The same circuit through fused passes, complex128 and complex64, and as
+    a subcircuit file (chunk_groups, 12-qubit chunks) through the subcircuit
+    path; each is compared with the exact per-gate complex128 state left in
+    `exact`."""
     import torch
     from subquokka_dev_b200 import Plan, StateVector
     out = {}
     n = args.qubits
+    from subquokka_dev_b200 import chunk_groups
+    sub = chunk_groups(circ, n, 12)   # the circuit as a subcircuit file, 12-qubit chunks
     for key, dtype, fw in (("c128", "c128", 0), ("c64", "c64", 0), ("c64_tensor_core", "c64", 6),
-                           ("c64_tensor_core_width5", "c64", 5)):
-        plan = Plan(circ, n, dtype, fuse_width=fw)
+                           ("c64_tensor_core_width5", "c64", 5), ("c128_subcircuit_file", "c128", -1),
+                           ("c64_subcircuit_file", "c64", -1)):
+        plan = Plan(sub, n, dtype, groups=True) if fw < 0 else Plan(circ, n, dtype, fuse_width=fw)
         passes, ops, remaps = plan.stats()
         sv = StateVector(n, dtype)
         sv.set_stream(torch.cuda.current_stream().cuda_stream)
@@ -284,13 +289,15 @@ def fused_variants(args, circ, exact, plain_ms, alg):
 
 def extra_workloads(args):
     """The other named workloads, each timed with CUDA events after warm-up:
-    QFT-20 on a seeded random state; the 26-qubit hardware-efficient ansatz
+    QFT-20 on a seeded random state; QFT-30 as a subcircuit file through the
+    subcircuit path against its flat fused plan; the 26-qubit hardware-efficient ansatz
     (12 layers, 624 parameters, ZZ + X Hamiltonian): <H> + adjoint gradient;
     the 33-qubit 24-layer random circuit in complex64 (fused passes), its error
     measured against complex128 on the same circuit family at 28 qubits."""
     import numpy as np
     import torch
-    from subquokka_dev_b200 import Circuit, Plan, StateVector, adjoint_grad, circuits, make_gate, zz_x_hamiltonian
+    from subquokka_dev_b200 import (Circuit, Plan, StateVector, adjoint_grad, chunk_groups, circuits, make_gate,
+                                    zz_x_hamiltonian)
     from subquokka_dev_b200.torch_shim import hea_template
     out = {}
     stream = torch.cuda.current_stream().cuda_stream
@@ -314,6 +321,33 @@ def extra_workloads(args):
                          "gates_per_s_per_gate_graph": qft.ngates / (ms_gr / 1e3)}
     sv.close()
     plan.close()
+
+    # QFT-30 as a subcircuit file (12-qubit chunks, VSWAP groups between the
+    # compute groups, written by chunk_groups) through the subcircuit path,
+    # against the flat circuit's fused plan
+    n = 30
+    qft = circuits.qft(n)
+    sub = chunk_groups(qft, n, 12)
+    nv = sum(1 for i in range(sub.ngates) if sub.gates[i].kind == 14)
+    res = {"gates": qft.ngates, "chunk_qbit": 12, "groups": sub.ngroups, "vswaps_in_file": nv}
+    states = {}
+    for dtype in ("c128", "c64"):
+        sv = StateVector(n, dtype)
+        sv.set_stream(stream)
+        for key, plan in (("subcircuit_file", Plan(sub, n, dtype, groups=True)), ("flat_plan", Plan(qft, n, dtype))):
+            def run():
+                sv.reset()
+                plan.apply(sv)
+            ms = time_device(run, 2, max(1, min(args.steps, 5)))
+            res[f"{dtype}_{key}_ms"] = ms
+            res[f"{dtype}_{key}_passes"] = plan.stats()[0]
+            plan.close()
+            if dtype == "c128":
+                states[key] = sv.download()
+        sv.close()
+    res["max_abs_diff_file_vs_flat_c128"] = float(np.abs(states["subcircuit_file"] - states["flat_plan"]).max())
+    del states
+    out["qft30_subcircuit_file"] = res
 
     # HEA-26 adjoint gradients
     n, layers = 26, 12

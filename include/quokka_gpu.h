@@ -192,10 +192,15 @@ int qk_sv_release_workspace(qk_sv *sv);
 int qk_apply_gates(qk_sv *sv, const qk_gate *gates, size_t n);
 
 /* Subcircuit path: gates are split into consecutive groups of
- * group_sizes[0..ngroups) gates.  A group whose first gate is a VSWAP is a
- * qubit permutation; any other group is applied in one shared-memory-resident
- * pass over the state.  Replaces MEM_Runner::run(std::vector<std::vector<
- * Gate*>>&) (src/MEM_Runner.cpp:136-185).  Asynchronous on the state's stream. */
+ * group_sizes[0..ngroups) gates.  The result is the state the reference's
+ * subcircuit runner computes, with fewer state sweeps:
+ * - VSWAP groups move no amplitudes: they rename the qubits of the gates
+ *   after them, and one or two permutation rounds at the end bring the state
+ *   into the file's layout;
+ * - the gates of all other groups are fused into shared-memory-resident
+ *   passes as qk_plan_create fuses a flat list, across group bounds.
+ * Replaces MEM_Runner::run(std::vector<std::vector<Gate*>>&)
+ * (src/MEM_Runner.cpp:136-185).  Asynchronous on the state's stream. */
 int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes, size_t ngroups);
 
 /* Per-gate path on caller-owned device memory (for example a torch tensor):
@@ -245,10 +250,13 @@ typedef struct qk_plan qk_plan;
  * registers.  This replaces the reference's two-step recipe -- group gates
  * into 12-qubit chunks with subcircuitFinder (subcircuitFinder/finder.cpp:
  * 629-698) and run the groups chunk by chunk (src/MEM_Runner.cpp:172-183) --
- * for any circuit, with no VSWAP: a tile's qubits need not be contiguous. */
+ * for any circuit, with no VSWAP: a tile's qubits need not be contiguous.
+ * VSWAP gates of the list rename qubits instead of moving amplitudes, and so
+ * do SWAP gates when that gives fewer passes; a final permutation restores
+ * the layout. */
 int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_opts *opts, qk_plan **out);
-/* One pass per group of a subcircuit file (groups that do not fit one tile
- * are split); VSWAP groups become permutation passes. */
+/* The plan of a subcircuit file that qk_apply_groups runs: the gates of all
+ * groups fused as one list, VSWAPs as renamings of the qubits after them. */
 int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size_t ngroups, int nqubits,
                           const qk_plan_opts *opts, qk_plan **out);
 /* Number of passes, program operations and register re-mappings. */

@@ -7,7 +7,8 @@
 // (src/MEM_Runner.cpp:172-183).  Here the chunk is a tile of 2^T amplitudes
 // whose index bits can be ANY T qubits (the low ones for coalescing plus the
 // ones the gates need), so no VSWAP is needed: a pass gathers the strided
-// amplitude sets of its tiles straight from HBM.
+// amplitude sets of its tiles straight from HBM.  VSWAPs that a circuit (a
+// subcircuit file) does contain become renamings (relabel_perms).
 //
 // build_plan: greedy passes.  Walk the remaining gates in order; a gate joins
 // the current pass if none of its qubits is blocked (an earlier gate on that
