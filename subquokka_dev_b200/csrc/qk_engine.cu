@@ -23,6 +23,7 @@ struct DevPlan;
 void release_scratch_plan(DevPlan &dp);
 int apply_group_plan(qk_sv *sv, const qk_gate *gates, const int32_t *sizes, size_t ngroups);
 int apply_perm_gate(void *state, int n, int dtype, const Op &op, cudaStream_t st);
+int plan_prepare(qk_sv *sv, qk_plan *p);
 }  // namespace qk
 
 // qk_pass.cu's DevPlan, defined there; the state keeps one as scratch for the
@@ -380,10 +381,17 @@ int qk_apply_groups(qk_sv *sv, const qk_gate *gates, const int32_t *group_sizes,
 
 int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds) {
     if (!cfg || !c || !sv) return fail(QK_ERR_ARG, "null argument");
-    // fuse_width > 0 on a flat circuit: fused plan (built before the timed span,
-    // like the reference's parsing)
+    // fuse_width > 0 on a flat circuit: fused plan; a subcircuit file: its
+    // group plan.  Both are built before the timed span, like the reference's
+    // parsing.
     qk_plan *plan = nullptr;
-    if (cfg->fuse_width > 0 && !cfg->is_subcircuit) {
+    if (cfg->is_subcircuit) {
+        qk_plan_opts o;
+        std::memset(&o, 0, sizeof o);
+        o.dtype = sv->dtype;
+        int rc = qk_plan_create_groups(c->gates.data(), c->group_sizes.data(), c->group_sizes.size(), sv->n, &o, &plan);
+        if (rc) return rc;
+    } else if (cfg->fuse_width > 0) {
         qk_plan_opts o;
         std::memset(&o, 0, sizeof o);
         o.dtype = sv->dtype;
@@ -391,13 +399,18 @@ int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds
         int rc = qk_plan_create(c->gates.data(), c->gates.size(), sv->n, &o, &plan);
         if (rc) return rc;
     }
+    if (plan) {
+        int rc = qk::plan_prepare(sv, plan);
+        if (rc) {
+            qk_plan_destroy(plan);
+            return rc;
+        }
+    }
     cudaEvent_t t0, t1;
     QK_CUDA(cudaEventCreate(&t0));
     QK_CUDA(cudaEventCreate(&t1));
     QK_CUDA(cudaEventRecord(t0, sv->stream));
-    int rc = plan ? qk_plan_apply(sv, plan)
-             : cfg->is_subcircuit ? qk_apply_groups(sv, c->gates.data(), c->group_sizes.data(), c->group_sizes.size())
-                                  : qk_apply_gates(sv, c->gates.data(), c->gates.size());
+    int rc = plan ? qk_plan_apply(sv, plan) : qk_apply_gates(sv, c->gates.data(), c->gates.size());
     if (!rc) {
         cudaError_t e = cudaEventRecord(t1, sv->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(t1);

@@ -430,30 +430,50 @@ int qk_plan_stats(const qk_plan *p, size_t *passes, size_t *program_ops, size_t 
     return QK_OK;
 }
 
+}  // extern "C"
+
+namespace qk {
+// Device copies of a plan's programs (or tensor-core operands), made once;
+// qk_plan_apply calls it, qk_run calls it before its timed span.
+int plan_prepare(qk_sv *sv, qk_plan *p) {
+    if (p->uploaded) return QK_OK;
+    if (p->dense) {
+        std::vector<uint16_t> all, one;
+        for (const auto &b : p->blocks) {
+            if (b.perm) one.assign(2 * 128 * 128, 0);
+            else dense_block_operand(b, one);
+            all.insert(all.end(), one.begin(), one.end());
+        }
+        cudaError_t e = cudaMalloc(&p->dA, std::max<size_t>(1, all.size()) * sizeof(uint16_t));
+        if (e == cudaSuccess) e = cudaMalloc(&p->derr, sizeof(int));
+        if (e == cudaSuccess && !all.empty())
+            e = cudaMemcpy(p->dA, all.data(), all.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_err(e, "upload dense blocks");
+    } else {
+        int rc = upload_plan(p->hp, p->hp.dtype, p->dp, state_stream(sv));
+        if (rc) return rc;
+        cudaError_t e = cudaStreamSynchronize(state_stream(sv));
+        if (e != cudaSuccess) return cuda_err(e, "plan upload");
+    }
+    p->uploaded = true;
+    return QK_OK;
+}
+}  // namespace qk
+
+extern "C" {
+
 int qk_plan_apply(qk_sv *sv, qk_plan *p) {
     if (!sv || !p) return fail(QK_ERR_ARG, "null argument");
     if (state_qubits(sv) != p->hp.n || state_dtype(sv) != p->hp.dtype)
         return fail(QK_ERR_ARG, "plan built for %d qubits dtype %d, state has %d qubits dtype %d", p->hp.n,
                     p->hp.dtype, state_qubits(sv), state_dtype(sv));
+    int rc = plan_prepare(sv, p);
+    if (rc) return rc;
     if (p->dense) {
         cudaStream_t st = state_stream(sv);
-        if (!p->uploaded) {
-            std::vector<uint16_t> all, one;
-            for (const auto &b : p->blocks) {
-                if (b.perm) one.assign(2 * 128 * 128, 0);
-                else dense_block_operand(b, one);
-                all.insert(all.end(), one.begin(), one.end());
-            }
-            cudaError_t e = cudaMalloc(&p->dA, std::max<size_t>(1, all.size()) * sizeof(uint16_t));
-            if (e == cudaSuccess) e = cudaMalloc(&p->derr, sizeof(int));
-            if (e == cudaSuccess && !all.empty())
-                e = cudaMemcpy(p->dA, all.data(), all.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
-            if (e != cudaSuccess) return cuda_err(e, "upload dense blocks");
-            p->uploaded = true;
-        }
         cudaError_t e = cudaMemsetAsync(p->derr, 0, sizeof(int), st);
         if (e != cudaSuccess) return cuda_err(e, "reset error flag");
-        int rc = run_dense_blocks(state_ptr(sv), p->hp.n, p->blocks, p->dA, p->derr, st);
+        rc = run_dense_blocks(state_ptr(sv), p->hp.n, p->blocks, p->dA, p->derr, st);
         if (rc) return rc;
         int herr = 0;
         e = cudaMemcpyAsync(&herr, p->derr, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -462,13 +482,6 @@ int qk_plan_apply(qk_sv *sv, qk_plan *p) {
         if (herr == 2) return fail(QK_ERR_CUDA, "tensor-core pass: shared memory not 1024-byte aligned");
         if (herr) return fail(QK_ERR_CUDA, "a tensor-core pass gave up waiting for its contraction");
         return QK_OK;
-    }
-    if (!p->uploaded) {
-        int rc = upload_plan(p->hp, p->hp.dtype, p->dp, state_stream(sv));
-        if (rc) return rc;
-        cudaError_t e = cudaStreamSynchronize(state_stream(sv));
-        if (e != cudaSuccess) return cuda_err(e, "plan upload");
-        p->uploaded = true;
     }
     return run_plan(state_ptr(sv), p->hp.dtype, p->hp, p->dp, state_stream(sv));
 }
