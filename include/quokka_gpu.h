@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define QK_ABI_VERSION 1
+#define QK_ABI_VERSION 2   /* 2: qk_config.init_file */
 #define QK_MAX_TARGETS 12
 
 /* Status codes.  The reference reports errors by printing to cerr and calling
@@ -101,6 +101,9 @@ typedef struct qk_config {
     int32_t dump_binary;      /* dump_format=bin -> 1, default 0 (text)      */
     char runner_type[32];     /* runner_type, default "IO"; "GPU" selects us */
     char dump_file[256];      /* dump_file, default ""                       */
+    char init_file[256];      /* init_file, default "": a state file
+                                 (qk_sv_load) to start from instead of
+                                 |0...0>                                     */
 } qk_config;
 
 typedef struct qk_circuit qk_circuit;   /* parsed gate list (+ group sizes) */
@@ -172,6 +175,13 @@ int qk_sv_reset(qk_sv *sv);
  * complex64 state the values are converted on the device. */
 int qk_sv_upload(qk_sv *sv, const double *host_c128);
 int qk_sv_download(qk_sv *sv, double *host_c128);
+/* Write / read a state file: raw little-endian complex128, 2^n interleaved
+ * (re, im) pairs (16 * 2^n bytes), the layout of dump_format=bin.  A
+ * complex64 state is widened on write and rounded on read; a file of any
+ * other size is refused.  The reference writes only its text dump
+ * (src/simulator.cpp:696-704) and reads no state. */
+int qk_sv_save(qk_sv *sv, const char *path);
+int qk_sv_load(qk_sv *sv, const char *path);
 /* Shape, type, device pointer and byte size of a state. */
 int qk_sv_info(const qk_sv *sv, int *nqubits, int *dtype, void **device_ptr, size_t *bytes);
 /* Order the state's work on a caller's cudaStream_t (NULL = default). */

@@ -17,6 +17,8 @@ QK_MAX_TARGETS = 12
 QK_C128, QK_C64 = 0, 1
 
 # qk_gate_kind
+ABI_VERSION = 2   # QK_ABI_VERSION of include/quokka_gpu.h that QkGate / QkConfig below mirror
+
 GATE_KINDS = {
     "H": 1, "X": 2, "Y": 3, "Z": 4, "P": 5, "RX": 6, "RY": 7, "RZ": 8,
     "U1": 9, "U2": 10, "SWAP": 11, "CP": 12, "RZZ": 13, "VSWAP": 14, "MPI_VSWAP": 15,
@@ -53,6 +55,7 @@ class QkConfig(ctypes.Structure):
         ("dump_binary", c_int32),
         ("runner_type", c_char * 32),
         ("dump_file", c_char * 256),
+        ("init_file", c_char * 256),
     ]
 
 
@@ -99,6 +102,8 @@ PROTOTYPES = {
     "qk_sv_reset": (c_int, [c_void_p]),
     "qk_sv_upload": (c_int, [c_void_p, POINTER(c_double)]),
     "qk_sv_download": (c_int, [c_void_p, POINTER(c_double)]),
+    "qk_sv_save": (c_int, [c_void_p, c_char_p]),
+    "qk_sv_load": (c_int, [c_void_p, c_char_p]),
     "qk_sv_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_void_p), POINTER(c_size_t)]),
     "qk_sv_set_stream": (c_int, [c_void_p, c_void_p]),
     "qk_sv_synchronize": (c_int, [c_void_p]),
@@ -152,6 +157,9 @@ def load() -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.qk_abi_version() != ABI_VERSION:   # the structures above must match the library's
+        raise RuntimeError(f"{LIB_PATH} has ABI version {lib.qk_abi_version()}, these bindings {ABI_VERSION}: "
+                           "rebuild it with `python -m subquokka_dev_b200.build`")
     _lib = lib
     return lib
 

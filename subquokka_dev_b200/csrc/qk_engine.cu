@@ -257,6 +257,67 @@ int qk_sv_download(qk_sv *sv, double *host) {
     return rc;
 }
 
+int qk_sv_save(qk_sv *sv, const char *path) {
+    if (!sv || !path) return fail(QK_ERR_ARG, "null argument");
+    const uint64_t namp = 1ull << sv->n;
+    const uint64_t chunk = std::min<uint64_t>(namp, 1ull << 22);   // 64 MiB of complex128
+    std::vector<double2> host(chunk);
+    double2 *tmp = nullptr;
+    if (sv->dtype == QK_C64) QK_CUDA(cudaMalloc(&tmp, chunk * sizeof(double2)));
+    FILE *f = std::fopen(path, "wb");
+    int rc = f ? QK_OK : fail(QK_ERR_IO, "cannot open %s for writing", path);
+    for (uint64_t off = 0; off < namp && !rc; off += chunk) {
+        const double2 *src = (const double2 *)sv->d + off;
+        if (tmp) {
+            k_c64_to_c128<<<(unsigned)((chunk + 255) / 256), 256, 0, sv->stream>>>((const float2 *)sv->d + off, tmp, chunk);
+            src = tmp;
+        }
+        cudaError_t e = cudaMemcpyAsync(host.data(), src, chunk * sizeof(double2), cudaMemcpyDeviceToHost, sv->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "save");
+        else if (std::fwrite(host.data(), sizeof(double2), chunk, f) != chunk) rc = fail(QK_ERR_IO, "cannot write %s", path);
+    }
+    if (f && std::fclose(f) != 0 && !rc) rc = fail(QK_ERR_IO, "cannot write %s", path);
+    if (tmp) cudaFree(tmp);
+    if (!rc) clear_error();
+    return rc;
+}
+
+int qk_sv_load(qk_sv *sv, const char *path) {
+    if (!sv || !path) return fail(QK_ERR_ARG, "null argument");
+    const uint64_t namp = 1ull << sv->n;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(QK_ERR_IO, "cannot open state file %s", path);
+    int rc = QK_OK;
+    if (std::fseek(f, 0, SEEK_END) != 0 || (uint64_t)std::ftell(f) != namp * sizeof(double2))
+        rc = fail(QK_ERR_ARG, "state file %s does not hold %llu complex128 amplitudes", path,
+                  (unsigned long long)namp);
+    std::rewind(f);
+    const uint64_t chunk = std::min<uint64_t>(namp, 1ull << 22);
+    std::vector<double2> host(chunk);
+    double2 *tmp = nullptr;
+    if (!rc && sv->dtype == QK_C64) {
+        cudaError_t e = cudaMalloc(&tmp, chunk * sizeof(double2));
+        if (e != cudaSuccess) rc = cuda_fail(e, "load");
+    }
+    for (uint64_t off = 0; off < namp && !rc; off += chunk) {
+        if (std::fread(host.data(), sizeof(double2), chunk, f) != chunk) {
+            rc = fail(QK_ERR_IO, "cannot read %s", path);
+            break;
+        }
+        double2 *dst = tmp ? tmp : (double2 *)sv->d + off;
+        cudaError_t e = cudaMemcpyAsync(dst, host.data(), chunk * sizeof(double2), cudaMemcpyHostToDevice, sv->stream);
+        if (e == cudaSuccess && tmp)
+            k_c128_to_c64<<<(unsigned)((chunk + 255) / 256), 256, 0, sv->stream>>>(tmp, (float2 *)sv->d + off, chunk);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);   // host buffer reused next chunk
+        if (e != cudaSuccess) rc = cuda_fail(e, "load");
+    }
+    std::fclose(f);
+    if (tmp) cudaFree(tmp);
+    if (!rc) clear_error();
+    return rc;
+}
+
 int qk_sv_info(const qk_sv *sv, int *nqubits, int *dtype, void **device_ptr, size_t *bytes) {
     if (!sv) return fail(QK_ERR_ARG, "null state");
     if (nqubits) *nqubits = sv->n;

@@ -454,6 +454,7 @@ int qk_config_load(const char *ini_path, qk_config *out) {
     else return fail(QK_ERR_ARG, "precision must be c128 or c64, got '%s'", prec.c_str());
     c.fuse_width = (int32_t)ini.get_int(S, "fuse_width", 0);
     c.dump_binary = lower(ini.get(S, "dump_format", "txt")) == "bin";
+    std::snprintf(c.init_file, sizeof c.init_file, "%s", ini.get(S, "init_file", "").c_str());
     // the reference's asserts (src/simulator.cpp:98-99, :152)
     const int n_local = c.total_qbit - c.mpi_qbit;
     if (c.chunk_qbit < 1) return fail(QK_ERR_ARG, "chunk_qbit must be >= 1 (got %d)", c.chunk_qbit);

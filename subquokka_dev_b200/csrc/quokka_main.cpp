@@ -76,6 +76,7 @@ int main(int argc, char *argv[]) {
 
     qk_sv *sv = nullptr;
     if (qk_sv_create(cfg.total_qbit, cfg.precision, &sv)) return die("[GPU_Runner]");
+    if (cfg.init_file[0] && qk_sv_load(sv, cfg.init_file)) return die("[init_file]");
     std::cerr << "[Simulator]: Ready to go." << std::endl;
 
     double sec = 0;
@@ -83,23 +84,16 @@ int main(int argc, char *argv[]) {
     std::cout << sec << "s" << std::endl;
 
     const std::string dump = cfg.dump_file;
-    if (!dump.empty() && (cfg.MPI_testing || cfg.dump_binary)) {
+    if (!dump.empty() && cfg.dump_binary) {
+        if (qk_sv_save(sv, dump.c_str())) return die("[dump]");
+    } else if (!dump.empty() && cfg.MPI_testing) {
+        // the reference's text dump: name = dump_file[0:3] + rank + ".txt",
+        // one "%.11f" line per real and imaginary part (src/simulator.cpp:696-704)
         std::vector<double> host((size_t)2 << cfg.total_qbit);
         if (qk_sv_download(sv, host.data())) return die("[dump]");
-        if (cfg.dump_binary) {
-            FILE *f = std::fopen(dump.c_str(), "wb");
-            if (!f || std::fwrite(host.data(), sizeof(double), host.size(), f) != host.size()) {
-                std::cerr << "[dump]: cannot write " << dump << std::endl;
-                return 1;
-            }
-            std::fclose(f);
-        } else {
-            // the reference's text dump: name = dump_file[0:3] + rank + ".txt",
-            // one "%.11f" line per real and imaginary part (src/simulator.cpp:696-704)
-            std::ofstream res(dump.substr(0, 3) + "0.txt");
-            for (size_t k = 0; k < host.size(); k += 2)
-                res << std::fixed << std::setprecision(11) << host[k] << "\n" << host[k + 1] << "\n";
-        }
+        std::ofstream res(dump.substr(0, 3) + "0.txt");
+        for (size_t k = 0; k < host.size(); k += 2)
+            res << std::fixed << std::setprecision(11) << host[k] << "\n" << host[k + 1] << "\n";
     }
     qk_sv_destroy(sv);
     qk_circuit_destroy(c);

@@ -230,6 +230,14 @@ class StateVector:
         check(self._lib.qk_sv_download(self.h, out.ctypes.data_as(POINTER(c_double))))
         return out
 
+    def save(self, path: str) -> None:
+        """Write the state as raw little-endian complex128 (dump_format=bin)."""
+        check(self._lib.qk_sv_save(self.h, str(path).encode()))
+
+    def load(self, path: str) -> None:
+        """Read a state file written by save() or dump_format=bin."""
+        check(self._lib.qk_sv_load(self.h, str(path).encode()))
+
     def set_stream(self, stream_ptr: int | None) -> None:
         check(self._lib.qk_sv_set_stream(self.h, c_void_p(stream_ptr or 0)))
 
@@ -476,6 +484,8 @@ class Simulator:
             raise _lib.QkError(-8, "mpi_qbit > 0 is not supported by the GPU runner")
         self.circuit = Circuit.load(cir, self.config.is_subcircuit, self.config.total_qbit)
         self.state = StateVector(self.config.total_qbit, self.config.precision)
+        if self.config.init_file:
+            self.state.load(self.config.init_file)
 
     def run(self) -> float:
         sec = c_double()

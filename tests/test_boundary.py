@@ -29,13 +29,13 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) <= set(_lib.PROTOTYPES), set(names) - set(_lib.PROTOTYPES)
-    assert lib.qk_abi_version() == 1
+    assert lib.qk_abi_version() == 2
 
 
 def test_struct_layouts_match_header():
     import ctypes
     assert ctypes.sizeof(_lib.QkGate) == 4 + 4 + 4 * 12 + 8 + 8 * 32
-    assert ctypes.sizeof(_lib.QkConfig) == 10 * 4 + 32 + 256
+    assert ctypes.sizeof(_lib.QkConfig) == 10 * 4 + 32 + 256 + 256
 
 
 def write(tmp_path, name, text):
@@ -50,7 +50,12 @@ def test_ini_defaults_and_keys(tmp_path):
     c = Config(ini)
     assert (c.total_qbit, c.mpi_qbit, c.file_qbit, c.chunk_qbit) == (20, 0, 3, 12)
     assert c.is_subcircuit == 1 and c.MPI_buffe_size == 16 and c.MPI_testing == 0
-    assert c.runner_type == "GPU" and c.dump_file == "" and c.precision == 0
+    assert c.runner_type == "GPU" and c.dump_file == "" and c.precision == 0 and c.init_file == ""
+
+
+def test_ini_init_file_key(tmp_path):
+    ini = write(tmp_path, "i.ini", "[system]\ntotal_qbit=8\nchunk_qbit=4\ninit_file=/data/start.bin\n")
+    assert Config(ini).init_file == "/data/start.bin"
 
 
 def test_ini_comments_case_and_engine_keys(tmp_path):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
-from subquokka_dev_b200 import Circuit, StateVector, apply_gates_dev, chunk_groups, circuits, make_gate
+from subquokka_dev_b200 import Circuit, QkError, StateVector, apply_gates_dev, chunk_groups, circuits, make_gate
 
 import golden_util as gu
 
@@ -202,6 +202,40 @@ def test_cli_dump_matches_reference_golden(tmp_path):
     z = np.zeros(1 << rec["n"], np.complex128)
     z[0] = 1
     assert np.abs(out - oracle.apply_circuit(z, rec["n"], circ)).max() <= TOL_C128
+
+
+@pytest.mark.parametrize("name", ["sub12", "rand10", "sub21"])
+def test_cli_init_file_reproduces_reference_golden(tmp_path, name):
+    # the fixture's own seeded initial state as init_file (raw complex128),
+    # its circuit through the CLI, the final state against the reference's
+    rec = gu.load(name)
+    init = gu.initial_state(rec)
+    init.astype(np.complex128).tofile(tmp_path / "init.bin")
+    ini = tmp_path / "x.ini"
+    ini.write_text(f"[system]\ntotal_qbit={rec['n']}\nfile_qbit=0\nchunk_qbit=4\nrunner_type=GPU\n"
+                   f"is_subcircuit={rec['is_subcircuit']}\ninit_file={tmp_path}/init.bin\n"
+                   f"dump_file={tmp_path}/state.bin\ndump_format=bin\n")
+    (tmp_path / "c.txt").write_text(rec["circuit"])
+    r = subprocess.run([CLI, "-i", str(ini), "-c", str(tmp_path / "c.txt")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert gu.compare(rec, np.fromfile(tmp_path / "state.bin", dtype=np.complex128)) <= TOL_C128
+
+
+@pytest.mark.parametrize("dtype,tol", [("c128", 0.0), ("c64", 2e-7)])
+def test_state_file_round_trip(tmp_path, dtype, tol):
+    n = 23   # two 2^22-amplitude chunks
+    init = circuits.random_state(n, 3)
+    with StateVector(n, dtype) as a, StateVector(n, dtype) as b:
+        a.upload(init)
+        a.save(tmp_path / "s.bin")
+        b.load(tmp_path / "s.bin")
+        assert np.abs(b.download() - a.download()).max() == 0
+        assert np.abs(np.fromfile(tmp_path / "s.bin", dtype=np.complex128) - init).max() <= tol
+    with StateVector(n - 1, dtype) as c:
+        with pytest.raises(QkError):
+            c.load(tmp_path / "s.bin")        # wrong size
+        with pytest.raises(QkError):
+            c.load(tmp_path / "missing.bin")
 
 
 def test_cli_text_dump_format(tmp_path):
