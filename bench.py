@@ -266,8 +266,9 @@ def fused_variants(args, circ, exact, plain_ms, alg):
     sub = chunk_groups(circ, n, 12)   # the circuit as a subcircuit file, 12-qubit chunks
     for key, dtype, fw in (("c128", "c128", 0), ("c64", "c64", 0), ("c64_tensor_core", "c64", 6),
                            ("c64_tensor_core_width5", "c64", 5), ("c128_subcircuit_file", "c128", -1),
-                           ("c64_subcircuit_file", "c64", -1)):
-        plan = Plan(sub, n, dtype, groups=True) if fw < 0 else Plan(circ, n, dtype, fuse_width=fw)
+                           ("c64_subcircuit_file", "c64", -1), ("c64_tensor_core_subcircuit_file", "c64", -6)):
+        plan = (Plan(sub, n, dtype, groups=True, fuse_width=-fw if fw < -1 else 0) if fw < 0
+                else Plan(circ, n, dtype, fuse_width=fw))
         passes, ops, remaps = plan.stats()
         sv = StateVector(n, dtype)
         sv.set_stream(torch.cuda.current_stream().cuda_stream)

@@ -95,9 +95,11 @@ typedef struct qk_config {
     int32_t MPI_testing;      /* MPI_testing, default 0                      */
     int32_t MPI_buffe_size;   /* MPI_buffe_size (sic), default 16            */
     int32_t precision;        /* precision=c128|c64 -> qk_dtype, default c128 */
-    int32_t fuse_width;       /* fuse_width, default 0: per-gate kernels; on a
-                                 flat circuit > 0 runs fused passes, 5 or 6
-                                 with precision=c64 tensor-core blocks       */
+    int32_t fuse_width;       /* fuse_width, default 0: per-gate kernels for a
+                                 flat circuit, fused passes for a subcircuit
+                                 file; > 0 fused passes for a flat circuit
+                                 too; 5 or 6 with precision=c64 tensor-core
+                                 blocks for either                           */
     int32_t dump_binary;      /* dump_format=bin -> 1, default 0 (text)      */
     char runner_type[32];     /* runner_type, default "IO"; "GPU" selects us */
     char dump_file[256];      /* dump_file, default ""                       */
@@ -266,7 +268,9 @@ typedef struct qk_plan qk_plan;
  * the layout. */
 int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_opts *opts, qk_plan **out);
 /* The plan of a subcircuit file that qk_apply_groups runs: the gates of all
- * groups fused as one list, VSWAPs as renamings of the qubits after them. */
+ * groups fused as one list, VSWAPs as renamings of the qubits after them.
+ * With opts->fuse_width 5 or 6 (complex64): tensor-core dense blocks over
+ * the same list, as qk_plan_create makes them. */
 int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size_t ngroups, int nqubits,
                           const qk_plan_opts *opts, qk_plan **out);
 /* Number of passes, program operations and register re-mappings. */

@@ -450,6 +450,7 @@ int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds
         qk_plan_opts o;
         std::memset(&o, 0, sizeof o);
         o.dtype = sv->dtype;
+        o.fuse_width = (cfg->fuse_width == 5 || cfg->fuse_width == 6) && sv->dtype == QK_C64 ? cfg->fuse_width : 0;
         int rc = qk_plan_create_groups(c->gates.data(), c->group_sizes.data(), c->group_sizes.size(), sv->n, &o, &plan);
         if (rc) return rc;
     } else if (cfg->fuse_width > 0) {

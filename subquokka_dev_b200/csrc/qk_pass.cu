@@ -402,6 +402,16 @@ int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size
                           const qk_plan_opts *opts, qk_plan **out) {
     if (!out || (!group_sizes && ngroups)) return fail(QK_ERR_ARG, "null argument");
     if (nqubits < 1 || nqubits > 36) return fail(QK_ERR_ARG, "nqubits must be in [1, 36], got %d", nqubits);
+    if (opts && opts->fuse_width) {
+        // tensor-core blocks: the groups' gates as one list (their VSWAPs
+        // become renamings inside build_dense_blocks)
+        size_t ng = 0;
+        for (size_t g = 0; g < ngroups; ++g) {
+            if (group_sizes[g] < 0) return fail(QK_ERR_ARG, "group %zu has negative size", g);
+            ng += (size_t)group_sizes[g];
+        }
+        return qk_plan_create(gates, ng, nqubits, opts, out);
+    }
     const int dtype = opts ? opts->dtype : QK_C128;
     PlanOptions o = default_plan_options(dtype, nqubits);
     if (opts && opts->tile_bits) o.tile_bits = opts->tile_bits;

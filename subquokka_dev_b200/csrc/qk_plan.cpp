@@ -53,6 +53,28 @@ namespace {
 
 int low_bits(int dtype) { return dtype == QK_C128 ? 3 : 4; }  // 128-byte runs
 
+// ASAP layers: level = 1 + the highest level on the op's qubits (a
+// permutation op takes every qubit's level); a stable sort by level keeps
+// each qubit's op order, so the list computes the same state.
+void asap_order(std::vector<Op> &ops, int n) {
+    std::vector<int> lvl(n, 0);
+    std::vector<std::pair<int, size_t>> key(ops.size());
+    for (size_t i = 0; i < ops.size(); ++i) {
+        const Op &op = ops[i];
+        const bool all = op.kind == OP_PERM;
+        int l = 0;
+        for (int k = 0; k < (all ? n : op.nq); ++k) l = std::max(l, lvl[all ? k : op.q[k]]);
+        ++l;
+        for (int k = 0; k < (all ? n : op.nq); ++k) lvl[all ? k : op.q[k]] = l;
+        key[i] = {l, i};
+    }
+    std::stable_sort(key.begin(), key.end());
+    std::vector<Op> sorted;
+    sorted.reserve(ops.size());
+    for (const auto &k : key) sorted.push_back(ops[k.second]);
+    ops.swap(sorted);
+}
+
 // Most tile bits of a permutation pass (qk_pass.cu stages such a tile in
 // shared memory in one buffer).
 int perm_tile_bits(int dtype) { return dtype == QK_C128 ? 13 : 14; }
@@ -509,11 +531,15 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
     // VSWAPs are always renamings.  SWAP gates are too when that gives fewer
     // passes: their renaming removes them from the compute passes but can
     // leave a longer permutation to restore at the end.
+    // The greedy planner follows list order: the list as given and its ASAP
+    // layering are both planned (2 ms for 900 gates), the one with fewer
+    // passes is kept.
     bool swaps = false;
     for (const Op &op : lowered) swaps = swaps || (op.kind == OP_SWAP2 && op.aux != 1);
-    for (int variant = 0; variant < (swaps ? 2 : 1); ++variant) {
+    for (int variant = 0; variant < (swaps ? 4 : 2); ++variant) {
         std::vector<Op> ops = lowered;
-        relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant == 1);
+        relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant >= 2);
+        if (variant % 2) asap_order(ops, n);
         HostPlan hp;
         hp.n = n;
         hp.dtype = o.dtype;
@@ -638,15 +664,9 @@ static void block_apply(std::vector<double> &u, const Op &op, const int *loc) {
     }
 }
 
-int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::vector<DenseBlock> &blocks) {
-    if (n < kDenseQubits) return fail(QK_ERR_ARG, "dense blocks need at least %d qubits", kDenseQubits);
-    if (width < 2 || width > kDenseQubits) return fail(QK_ERR_ARG, "block width must be in [2, %d], got %d", kDenseQubits, width);
-    std::vector<Op> ops;
-    int rc = lower_all(gates, ng, n, ops);
-    if (rc) return rc;
-    // at most three pairs per restoring permutation: a permutation block
-    // lists its targets in kDenseQubits entries
-    relabel_perms(ops, n, low_bits(QK_C64), perm_tile_bits(QK_C64), kDenseQubits / 2, false);
+// The block partition of an op list; with_u: also the blocks' unitaries.
+static void dense_partition(const std::vector<Op> &ops, int n, int width, bool with_u,
+                            std::vector<DenseBlock> &blocks) {
     blocks.clear();
     std::vector<size_t> pending(ops.size());
     for (size_t i = 0; i < ops.size(); ++i) pending[i] = i;
@@ -734,18 +754,41 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::v
         std::sort(Q.begin(), Q.end());
         DenseBlock b;
         for (int k = 0; k < kDenseQubits; ++k) b.q[k] = Q[k];
-        b.u.assign(2 * kDenseDim * kDenseDim, 0.0);
-        for (int k = 0; k < kDenseDim; ++k) b.u[2 * (k * kDenseDim + k)] = 1.0;
-        for (size_t i : take) {
-            int loc[QK_MAX_TARGETS];
-            for (int k = 0; k < ops[i].nq; ++k)
-                loc[k] = (int)(std::find(Q.begin(), Q.end(), ops[i].q[k]) - Q.begin());
-            block_apply(b.u, ops[i], loc);
+        if (with_u) {
+            b.u.assign(2 * kDenseDim * kDenseDim, 0.0);
+            for (int k = 0; k < kDenseDim; ++k) b.u[2 * (k * kDenseDim + k)] = 1.0;
+            for (size_t i : take) {
+                int loc[QK_MAX_TARGETS];
+                for (int k = 0; k < ops[i].nq; ++k)
+                    loc[k] = (int)(std::find(Q.begin(), Q.end(), ops[i].q[k]) - Q.begin());
+                block_apply(b.u, ops[i], loc);
+            }
         }
         b.ngates = (int)take.size();
         blocks.push_back(std::move(b));
         pending.swap(rest);
     }
+}
+
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::vector<DenseBlock> &blocks) {
+    if (n < kDenseQubits) return fail(QK_ERR_ARG, "dense blocks need at least %d qubits", kDenseQubits);
+    if (width < 2 || width > kDenseQubits) return fail(QK_ERR_ARG, "block width must be in [2, %d], got %d", kDenseQubits, width);
+    std::vector<Op> ops;
+    int rc = lower_all(gates, ng, n, ops);
+    if (rc) return rc;
+    // at most three pairs per restoring permutation: a permutation block
+    // lists its targets in kDenseQubits entries
+    relabel_perms(ops, n, low_bits(QK_C64), perm_tile_bits(QK_C64), kDenseQubits / 2, false);
+    // The fuser follows list order, so the same circuit in another valid
+    // order can need fewer blocks: the list as given and its ASAP layering
+    // are both partitioned, and the one with fewer blocks is kept (on the
+    // 26-qubit HEA 37 blocks instead of 55; QFTs keep their own order).
+    std::vector<Op> layered = ops;
+    asap_order(layered, n);
+    std::vector<DenseBlock> a, b;
+    dense_partition(ops, n, width, false, a);
+    dense_partition(layered, n, width, false, b);
+    dense_partition(b.size() < a.size() ? layered : ops, n, width, true, blocks);
     return QK_OK;
 }
 

@@ -146,6 +146,25 @@ def test_chunk_grouped_file_through_group_path(name, dtype, tol):
     assert np.abs(run_gpu(n, sub, init, dtype, groups=True) - ref).max() <= tol
 
 
+def test_chunk_grouped_file_on_tensor_cores():
+    # the same kind of file through tensor-core dense blocks (complex64,
+    # 3 x BF16): 1 - F <= 1e-6 against the flat circuit
+    from subquokka_dev_b200 import Plan
+    n = 20
+    circ = circuits.random_u3_cz(n, 8, 5)
+    sub = chunk_groups(circ, n, 12)
+    init = circuits.random_state(n, 13)
+    ref = oracle.apply_circuit(init, n, circ)
+    plan = Plan(sub, n, "c64", groups=True, fuse_width=6)
+    with StateVector(n, "c64") as sv:
+        sv.upload(init)
+        plan.apply(sv)
+        out = sv.download()
+    plan.close()
+    ov = np.vdot(ref, out)
+    assert 1 - abs(ov) ** 2 / (np.vdot(out, out).real * np.vdot(ref, ref).real) <= 1e-6
+
+
 def inverse(circ):
     out = []
     for g in reversed(circ.gate_list()):

@@ -107,6 +107,29 @@ def test_dense_fuser_blocks_reproduce_the_circuit(seed, width):
     assert np.abs(out - oracle.apply_circuit(s, n, circ)).max() < 1e-12
 
 
+def test_dense_blocks_of_a_subcircuit_file_reproduce_the_circuit():
+    # a chunk-grouped file's VSWAPs become renamings inside the dense-block
+    # fuser; replaying its blocks (permutation blocks as VSWAPs) on the CPU
+    # gives the flat circuit's state
+    import oracle
+    n = 13
+    circ = circuits.random_u3_cz(n, 6, 4)
+    sub = sq.chunk_groups(circ, n, 5)
+    p = Plan(sub, n, "c64", groups=True, fuse_width=6)
+    s = circuits.random_state(n, 6)
+    out = s.copy()
+    nperm = 0
+    for k in range(p.stats()[0]):
+        qs, u, perm = p.dense_block(k)
+        if perm:
+            nperm += 1
+            out = oracle.apply_circuit(out, n, Circuit([make_gate("VSWAP", qs)]))
+        else:
+            out = apply_block(out, n, qs, u)
+    assert nperm <= 2 * 6          # the final restore only, at most two rounds
+    assert np.abs(out - oracle.apply_circuit(s, n, circ)).max() < 1e-12
+
+
 def test_fuse_width_must_be_5_or_6():
     c = circuits.random_u3_cz(14, 2, 3)
     for w in (1, 4, 7):
