@@ -602,14 +602,26 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
         invert_op(op);
         ops.push_back(op);
     }
-    plan = HostPlan();
-    plan.n = n;
-    plan.dtype = o.dtype;
-    plan.T = o.tile_bits;
-    plan.r = o.reg_bits;
-    plan.nstates = 2;
-    PassBuilder b{ops, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), plan};
-    return b.greedy(0, ops.size());
+    // A gradient op only needs the ops on its own qubit in order: ops on
+    // other qubits act on both states alike and commute with G.  So the
+    // backward list may be layered too; the order with fewer passes is kept.
+    for (int variant = 0; variant < 2; ++variant) {
+        std::vector<Op> list = ops;
+        if (variant) asap_order(list, n);
+        HostPlan hp;
+        hp.n = n;
+        hp.dtype = o.dtype;
+        hp.T = o.tile_bits;
+        hp.r = o.reg_bits;
+        hp.nstates = 2;
+        PassBuilder b{list, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), hp};
+        rc = b.greedy(0, list.size());
+        if (rc) return rc;
+        if (variant == 0 || hp.passes.size() < plan.passes.size() ||
+            (hp.passes.size() == plan.passes.size() && hp.ops.size() < plan.ops.size()))
+            plan = std::move(hp);
+    }
+    return QK_OK;
 }
 
 // Apply a lowered op (dense matrix over its targets, little-endian) to the
