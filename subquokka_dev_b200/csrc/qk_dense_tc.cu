@@ -263,12 +263,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
 #pragma unroll
                 for (int u = 0; u < NU; ++u) {
                     const float2 *q = p + lrow + (u & 1 ? lu[0] : 0) + (u & 2 ? lu[1] : 0);
-                    const float4 v0 = *reinterpret_cast<const float4 *>(q);
-                    const float4 v1 = *reinterpret_cast<const float4 *>(q + lpair);
-                    x[4 * u + 0] = make_float2(v0.x, v0.y);
-                    x[4 * u + 1] = make_float2(v0.z, v0.w);
-                    x[4 * u + 2] = make_float2(v1.x, v1.y);
-                    x[4 * u + 3] = make_float2(v1.z, v1.w);
+                    if (lpair == 2 && (reinterpret_cast<uintptr_t>(q) & 31) == 0) {
+                        // block bits 0, 1 are state bits 0, 1: the chunk is one
+                        // 32-byte sector, read by one 256-bit load
+                        float r[8];
+                        asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                                     : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]),
+                                       "=f"(r[6]), "=f"(r[7])
+                                     : "l"(q));
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) x[4 * u + k] = make_float2(r[2 * k], r[2 * k + 1]);
+                    } else {
+                        const float4 v0 = *reinterpret_cast<const float4 *>(q);
+                        const float4 v1 = *reinterpret_cast<const float4 *>(q + lpair);
+                        x[4 * u + 0] = make_float2(v0.x, v0.y);
+                        x[4 * u + 1] = make_float2(v0.z, v0.w);
+                        x[4 * u + 2] = make_float2(v1.x, v1.y);
+                        x[4 * u + 3] = make_float2(v1.z, v1.w);
+                    }
                 }
             }
         };
