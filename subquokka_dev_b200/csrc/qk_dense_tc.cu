@@ -210,13 +210,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
+    // each CTA takes a contiguous range of supertiles: consecutive supertiles
+    // are neighbours along the lowest state bit outside the tile, so a CTA
+    // streams each of the block's 64 row runs forward instead of striding
+    const uint64_t o_lo = nsup * blockIdx.x / gridDim.x, o_hi = nsup * (blockIdx.x + 1) / gridDim.x;
 
     if (issuer) {
         // one thread issues every contraction: wait until buffer b is
         // converted and accumulator b drained, then 24 MMAs and a commit
         if (lane == 0) {
             uint32_t it = 0;
-            for (uint64_t o = blockIdx.x; o < nsup && !bad_s; o += gridDim.x, ++it) {
+            for (uint64_t o = o_lo; o < o_hi && !bad_s; ++o, ++it) {
                 const uint32_t b = it & 1;
                 if (!tc_wait(&full[b], (it >> 1) & 1u) || (it >= 2 && !tc_wait(&empty[b], ((it - 2) >> 1) & 1u))) {
                     bad_s = 1;
@@ -371,12 +375,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
         uint32_t it = 0;
         bool bad = false;
         float2 x[16];
-        uint64_t o = blockIdx.x, base = 0, prev = 0;
-        if (o < nsup) {
+        uint64_t o = o_lo, base = 0, prev = 0;
+        if (o < o_hi) {
             base = pass_base(o, d);
             load(x, s + base);
         }
-        for (; o < nsup; o += gridDim.x, ++it) {
+        for (; o < o_hi; ++o, ++it) {
             if (__shfl_sync(0xffffffffu, bad_s, 0)) {
                 bad = true;
                 break;
@@ -388,8 +392,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             arrive(&full[b]);
             const uint64_t cur = base;
-            if (o + gridDim.x < nsup) {
-                base = pass_base(o + gridDim.x, d);
+            if (o + 1 < o_hi) {
+                base = pass_base(o + 1, d);
                 load(x, s + base);
             }
             if (it > 0) {
