@@ -76,6 +76,66 @@ void asap_order(std::vector<Op> &ops, int n) {
     ops.swap(sorted);
 }
 
+// Consecutive one-qubit ops on the same qubit (no other op on that qubit
+// between them) multiplied into one: the later op moves back past ops on
+// other qubits, which commute with it.  Two diagonal ops give a diagonal op,
+// anything else a dense one.  Gradient ops and multi-qubit ops end a run.
+bool one_qubit(const Op &op) { return op.kind == OP_DENSE1 || op.kind == OP_PHASE1 || op.kind == OP_DIAG1; }
+
+void as_matrix(const Op &op, double (&m)[8]) {
+    std::memset(m, 0, sizeof m);
+    if (op.kind == OP_DENSE1) {
+        std::memcpy(m, op.m, sizeof m);
+    } else if (op.kind == OP_PHASE1) {
+        m[0] = 1;
+        m[6] = op.m[0];
+        m[7] = op.m[1];
+    } else {   // OP_DIAG1
+        m[0] = op.m[0];
+        m[1] = op.m[1];
+        m[6] = op.m[2];
+        m[7] = op.m[3];
+    }
+}
+
+void merge_one_qubit_runs(std::vector<Op> &ops, int n) {
+    std::vector<long> last(n, -1);
+    std::vector<Op> out;
+    out.reserve(ops.size());
+    for (const Op &op : ops) {
+        if (one_qubit(op) && last[op.q[0]] >= 0) {
+            Op &a = out[last[op.q[0]]];
+            double x[8], y[8], z[8];
+            as_matrix(a, x);
+            as_matrix(op, y);
+            for (int r = 0; r < 2; ++r)      // z = y x (op after a)
+                for (int c = 0; c < 2; ++c) {
+                    double re = 0, im = 0;
+                    for (int k = 0; k < 2; ++k) {
+                        const double yr = y[2 * (2 * r + k)], yi = y[2 * (2 * r + k) + 1];
+                        const double xr = x[2 * (2 * k + c)], xi = x[2 * (2 * k + c) + 1];
+                        re += yr * xr - yi * xi;
+                        im += yr * xi + yi * xr;
+                    }
+                    z[2 * (2 * r + c)] = re;
+                    z[2 * (2 * r + c) + 1] = im;
+                }
+            if (a.kind != OP_DENSE1 && op.kind != OP_DENSE1) {
+                a.kind = OP_DIAG1;
+                a.m[0] = z[0]; a.m[1] = z[1]; a.m[2] = z[6]; a.m[3] = z[7];
+            } else {
+                a.kind = OP_DENSE1;
+                std::memcpy(a.m, z, sizeof z);
+            }
+            continue;
+        }
+        for (int k = 0; k < op.nq; ++k) last[op.q[k]] = -1;
+        out.push_back(op);
+        if (one_qubit(op)) last[op.q[0]] = (long)out.size() - 1;
+    }
+    ops.swap(out);
+}
+
 // Most tile bits of a permutation pass (qk_pass.cu stages such a tile in
 // shared memory in one buffer).
 int perm_tile_bits(int dtype) { return dtype == QK_C128 ? 13 : 14; }
@@ -540,6 +600,7 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
     for (int variant = 0; variant < (swaps ? 4 : 2); ++variant) {
         std::vector<Op> ops = lowered;
         relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant >= 2);
+        merge_one_qubit_runs(ops, n);
         if (variant % 2) asap_order(ops, n);
         HostPlan hp;
         hp.n = n;
@@ -603,6 +664,7 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
         invert_op(op);
         ops.push_back(op);
     }
+    merge_one_qubit_runs(ops, n);   // between gradient ops only: they end a run
     // A gradient op only needs the ops on its own qubit in order: ops on
     // other qubits act on both states alike and commute with G.  So the
     // backward list may be layered too; the order with fewer passes is kept.
