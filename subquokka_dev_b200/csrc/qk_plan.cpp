@@ -22,6 +22,7 @@
 // can run the tile is re-distributed through shared memory (TOP_REMAP) so that
 // the qubits of the next ready gates become register bits.
 #include <algorithm>
+#include <array>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -132,6 +133,94 @@ void merge_one_qubit_runs(std::vector<Op> &ops, int n) {
         for (int k = 0; k < op.nq; ++k) last[op.q[k]] = -1;
         out.push_back(op);
         if (one_qubit(op)) last[op.q[0]] = (long)out.size() - 1;
+    }
+    ops.swap(out);
+}
+
+// 2 x 2 complex products, row-major (re, im) pairs.
+void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]) {   // z = x y
+    for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < 2; ++c) {
+            double re = 0, im = 0;
+            for (int k = 0; k < 2; ++k) {
+                const double xr = x[2 * (2 * r + k)], xi = x[2 * (2 * r + k) + 1];
+                const double yr = y[2 * (2 * k + c)], yi = y[2 * (2 * k + c) + 1];
+                re += xr * yr - xi * yi;
+                im += xr * yi + xi * yr;
+            }
+            z[2 * (2 * r + c)] = re;
+            z[2 * (2 * r + c) + 1] = im;
+        }
+}
+
+// Gradient ops of a backward sweep move to the start of their qubit's run of
+// one-qubit ops.  After ops U_1 .. U_k on that qubit (and any ops on other
+// qubits, which commute with G), Im<lambda|G|psi> equals Im<lambda|G'|psi>
+// before them with G' = P^dag G P, P = U_k ... U_1: a traceless Hermitian
+// a X + b Y + c Z (gen 4, a, b, c in m[2..4]).  The run's ops then follow
+// one another and merge_one_qubit_runs multiplies them into one.
+void hoist_gradients(std::vector<Op> &ops, int n) {
+    const size_t N = ops.size();
+    std::vector<long> start(n, -1);
+    std::vector<std::array<double, 8>> P(n);
+    std::vector<long> target(N, -1);
+    std::vector<Op> moved(ops);
+    for (size_t i = 0; i < N; ++i) {
+        const Op &op = ops[i];
+        if (op.kind == OP_GRAD) {
+            const int q = op.q[0];
+            if (start[q] < 0) continue;
+            target[i] = start[q];
+            double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            const int gen = (int)op.m[0];
+            if (gen == 1) { g[2] = 1; g[4] = 1; }
+            else if (gen == 2) { g[3] = -1; g[5] = 1; }
+            else if (gen == 3) { g[0] = 1; g[6] = -1; }
+            else { g[2] = op.m[2]; g[3] = -op.m[3]; g[4] = op.m[2]; g[5] = op.m[3]; g[0] = op.m[4]; g[6] = -op.m[4]; }
+            double pd[8], t[8], gp[8];
+            const auto &pm = P[q];
+            for (int r = 0; r < 2; ++r)   // P^dag
+                for (int c = 0; c < 2; ++c) {
+                    pd[2 * (2 * r + c)] = pm[2 * (2 * c + r)];
+                    pd[2 * (2 * r + c) + 1] = -pm[2 * (2 * c + r) + 1];
+                }
+            double pa[8];
+            for (int k = 0; k < 8; ++k) pa[k] = pm[k];
+            mat2_mul(pd, g, t);
+            mat2_mul(t, pa, gp);
+            Op &h = moved[i];
+            h.m[0] = 4;
+            h.m[2] = gp[4];   // a = Re G'10
+            h.m[3] = gp[5];   // b = Im G'10
+            h.m[4] = gp[0];   // c = Re G'00
+            continue;
+        }
+        if (one_qubit(op)) {
+            const int q = op.q[0];
+            double u[8], z[8];
+            as_matrix(op, u);
+            if (start[q] < 0) {
+                start[q] = (long)i;
+                for (int k = 0; k < 8; ++k) P[q][k] = u[k];
+            } else {
+                double pm[8];
+                for (int k = 0; k < 8; ++k) pm[k] = P[q][k];
+                mat2_mul(u, pm, z);
+                for (int k = 0; k < 8; ++k) P[q][k] = z[k];
+            }
+            continue;
+        }
+        const int nq = op.kind == OP_PERM ? n : op.nq;
+        for (int k = 0; k < nq; ++k) start[op.kind == OP_PERM ? k : op.q[k]] = -1;
+    }
+    std::vector<Op> out;
+    out.reserve(N);
+    std::vector<std::vector<size_t>> before(N);
+    for (size_t i = 0; i < N; ++i)
+        if (target[i] >= 0) before[target[i]].push_back(i);
+    for (size_t i = 0; i < N; ++i) {
+        for (size_t j : before[i]) out.push_back(moved[j]);
+        if (target[i] < 0) out.push_back(ops[i]);
     }
     ops.swap(out);
 }
@@ -263,7 +352,7 @@ struct PassBuilder {
         d.ngrad = (int)plan.grad_params.size() - d.grad0;
         // program coefficient indices relative to the pass's slice
         for (int i = d.prog0; i < d.prog0 + d.nprog; ++i)
-            if (plan.ops[i].kind != TOP_REMAP && plan.ops[i].kind != TOP_GRAD) plan.ops[i].coef -= (uint32_t)d.coef0;
+            if (plan.ops[i].kind != TOP_REMAP) plan.ops[i].coef -= (uint32_t)d.coef0;
         plan.passes.push_back(d);
         plan.ngates += idx.size();
         return QK_OK;
@@ -285,13 +374,20 @@ struct PassBuilder {
             for (int k = 0; k < 4; ++k) push_c(plan, op.m[2 * k], op.m[2 * k + 1]);
             break;
         case OP_GRAD: {
+            // gradient slot of the pass in bits[0..1]; a general generator
+            // (gen 4) as coefficients (a, b), (c, 0)
             t.kind = TOP_GRAD;
             t.a = (uint8_t)slot(op.q[0]);
             t.b = (uint8_t)op.m[0];
             int k = grad_base;
             while (k < (int)plan.grad_params.size() && plan.grad_params[k] != op.aux) ++k;
             if (k == (int)plan.grad_params.size()) plan.grad_params.push_back(op.aux);
-            t.coef = (uint32_t)(k - grad_base);
+            t.bits[0] = (uint8_t)((k - grad_base) & 0xFF);
+            t.bits[1] = (uint8_t)((k - grad_base) >> 8);
+            if (t.b == 4) {
+                push_c(plan, op.m[2], op.m[3]);
+                push_c(plan, op.m[4], 0);
+            }
             break;
         }
         case OP_DENSE2:
@@ -664,7 +760,8 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
         invert_op(op);
         ops.push_back(op);
     }
-    merge_one_qubit_runs(ops, n);   // between gradient ops only: they end a run
+    hoist_gradients(ops, n);
+    merge_one_qubit_runs(ops, n);
     // A gradient op only needs the ops on its own qubit in order: ops on
     // other qubits act on both states alike and commute with G.  So the
     // backward list may be layered too; the order with fewer passes is kept.
