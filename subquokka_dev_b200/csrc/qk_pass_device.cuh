@@ -272,15 +272,17 @@ __device__ __forceinline__ uint32_t reg_sidx(int kk, uint32_t stb, const uint32_
 // Im <lambda|G|psi> over this thread's register pairs of slot S, summed in
 // the state's precision (a thread holds at most 16 pairs).  G = X, Y, Z by
 // gen 1, 2, 3; gen 4: G = a X + b Y + c Z with (a, b) = g[0], (c, .) = g[1]
-// (a Pauli generator carried past one-qubit gates U as U^dag P U).
+// (a Pauli generator carried past one-qubit gates U as U^dag P U); gen 5: two
+// such generators (g[0..1], g[2..3]), the second sum in *s2.
 template <int S, typename C, int R>
-__device__ __forceinline__ auto reg_grad(const C (&v)[R], const C (&w)[R], int gen, const C *g) {
+__device__ __forceinline__ auto reg_grad(const C (&v)[R], const C (&w)[R], int gen, const C *g,
+                                         decltype(v[0].x) *s2) {
     using T = decltype(v[0].x);
     T s = 0;
     if constexpr ((1 << S) < R) {
         auto im = [](C l, C a) { return l.x * a.y - l.y * a.x; };
         auto re = [](C l, C a) { return l.x * a.x + l.y * a.y; };
-        if (gen == 4) {
+        if (gen >= 4) {
             T sx = 0, sy = 0, sz = 0;
 #pragma unroll
             for (int k = 0; k < R; ++k)
@@ -291,6 +293,7 @@ __device__ __forceinline__ auto reg_grad(const C (&v)[R], const C (&w)[R], int g
                     sz += im(w0, v0) - im(w1, v1);
                 }
             s = g[0].x * sx + g[0].y * sy + g[1].x * sz;
+            if (gen == 5) *s2 = g[2].x * sx + g[2].y * sy + g[3].x * sz;
         } else if (gen == 1) {
 #pragma unroll
             for (int k = 0; k < R; ++k)
@@ -451,18 +454,23 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             if constexpr (NS == 2) {
                 // summed over the warp in the state's precision, added to
                 // the CTA's double accumulator once per warp
-                decltype(v[0].x) g = 0;
+                decltype(v[0].x) g = 0, g2 = 0;
                 const C *gc = coef + op.coef;
                 switch (op.a) {
-                case 0: g = reg_grad<0>(v, w, op.b, gc); break;
-                case 1: g = reg_grad<1>(v, w, op.b, gc); break;
-                case 2: g = reg_grad<2>(v, w, op.b, gc); break;
-                case 3: g = reg_grad<3>(v, w, op.b, gc); break;
-                case 4: g = reg_grad<4>(v, w, op.b, gc); break;
+                case 0: g = reg_grad<0>(v, w, op.b, gc, &g2); break;
+                case 1: g = reg_grad<1>(v, w, op.b, gc, &g2); break;
+                case 2: g = reg_grad<2>(v, w, op.b, gc, &g2); break;
+                case 3: g = reg_grad<3>(v, w, op.b, gc, &g2); break;
+                case 4: g = reg_grad<4>(v, w, op.b, gc, &g2); break;
                 }
 #pragma unroll
                 for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
                 if ((tid & 31) == 0) atomicAdd(gsm + (op.bits[0] | (op.bits[1] << 8)), (double)g);
+                if (op.b == 5) {
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+                    if ((tid & 31) == 0) atomicAdd(gsm + (op.bits[2] | (op.bits[3] << 8)), (double)g2);
+                }
             }
             break;
         }

@@ -225,6 +225,44 @@ void hoist_gradients(std::vector<Op> &ops, int n) {
     ops.swap(out);
 }
 
+// Two gradient ops on the same qubit at the same point (next to each other
+// after hoist_gradients) share one sweep over the register pairs: gen 5
+// holds both generators, a1 b1 c1 in m[2..4] and a2 b2 c2 in m[5..7], the
+// second parameter index in m[8].
+void pair_gradients(std::vector<Op> &ops) {
+    auto abc = [](const Op &g, double *o) {
+        const int gen = (int)g.m[0];
+        o[0] = gen == 1 ? 1 : gen == 4 ? g.m[2] : 0;
+        o[1] = gen == 2 ? 1 : gen == 4 ? g.m[3] : 0;
+        o[2] = gen == 3 ? 1 : gen == 4 ? g.m[4] : 0;
+    };
+    std::vector<Op> out;
+    out.reserve(ops.size());
+    for (size_t i = 0; i < ops.size(); ++i) {
+        const Op &a = ops[i];
+        if (a.kind == OP_GRAD && (int)a.m[0] <= 4 && i + 1 < ops.size()) {
+            const Op &b = ops[i + 1];
+            if (b.kind == OP_GRAD && (int)b.m[0] <= 4 && b.q[0] == a.q[0]) {
+                Op p = a;
+                double x[3], y[3];
+                abc(a, x);
+                abc(b, y);
+                p.m[0] = 5;
+                for (int k = 0; k < 3; ++k) {
+                    p.m[2 + k] = x[k];
+                    p.m[5 + k] = y[k];
+                }
+                p.m[8] = b.aux;
+                out.push_back(p);
+                ++i;
+                continue;
+            }
+        }
+        out.push_back(a);
+    }
+    ops.swap(out);
+}
+
 // Most tile bits of a permutation pass (qk_pass.cu stages such a tile in
 // shared memory in one buffer).
 int perm_tile_bits(int dtype) { return dtype == QK_C128 ? 13 : 14; }
@@ -251,7 +289,12 @@ size_t op_cost(const Op &op, int dtype) {
     if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2) ncoef = 16;
     else if (op.kind == OP_PHASE1 || op.kind == OP_PHASE2) ncoef = 1;
     else if (op.kind == OP_CX) ncoef = 0;
-    else if (op.kind == OP_GRAD) return (16 + 8) * 5 / 4;  // one double accumulator
+    else if (op.kind == OP_GRAD) {
+        // one double accumulator per gradient; a general generator takes two
+        // coefficients, a pair of gradients four
+        const int gen = (int)op.m[0];
+        return (16 + (gen == 5 ? 16 + 4 * c : gen == 4 ? 8 + 2 * c : 8)) * 5 / 4;
+    }
     return (16 + ncoef * c) * 5 / 4;
 }
 
@@ -384,9 +427,19 @@ struct PassBuilder {
             if (k == (int)plan.grad_params.size()) plan.grad_params.push_back(op.aux);
             t.bits[0] = (uint8_t)((k - grad_base) & 0xFF);
             t.bits[1] = (uint8_t)((k - grad_base) >> 8);
-            if (t.b == 4) {
+            if (t.b == 4 || t.b == 5) {
                 push_c(plan, op.m[2], op.m[3]);
                 push_c(plan, op.m[4], 0);
+            }
+            if (t.b == 5) {   // the second gradient of the pair
+                const int32_t p2 = (int32_t)op.m[8];
+                int k2 = grad_base;
+                while (k2 < (int)plan.grad_params.size() && plan.grad_params[k2] != p2) ++k2;
+                if (k2 == (int)plan.grad_params.size()) plan.grad_params.push_back(p2);
+                t.bits[2] = (uint8_t)((k2 - grad_base) & 0xFF);
+                t.bits[3] = (uint8_t)((k2 - grad_base) >> 8);
+                push_c(plan, op.m[5], op.m[6]);
+                push_c(plan, op.m[7], 0);
             }
             break;
         }
@@ -762,6 +815,7 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
     }
     hoist_gradients(ops, n);
     merge_one_qubit_runs(ops, n);
+    pair_gradients(ops);
     // A gradient op only needs the ops on its own qubit in order: ops on
     // other qubits act on both states alike and commute with G.  So the
     // backward list may be layered too; the order with fewer passes is kept.
