@@ -468,11 +468,13 @@ int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds
             return rc;
         }
     }
-    cudaEvent_t t0, t1;
-    QK_CUDA(cudaEventCreate(&t0));
-    QK_CUDA(cudaEventCreate(&t1));
-    QK_CUDA(cudaEventRecord(t0, sv->stream));
-    int rc = plan ? qk_plan_apply(sv, plan) : qk_apply_gates(sv, c->gates.data(), c->gates.size());
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaError_t e0 = cudaEventCreate(&t0);
+    if (e0 == cudaSuccess) e0 = cudaEventCreate(&t1);
+    if (e0 == cudaSuccess) e0 = cudaEventRecord(t0, sv->stream);
+    int rc = e0 != cudaSuccess ? cuda_fail(e0, "timing events")
+             : plan            ? qk_plan_apply(sv, plan)
+                               : qk_apply_gates(sv, c->gates.data(), c->gates.size());
     if (!rc) {
         cudaError_t e = cudaEventRecord(t1, sv->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(t1);
@@ -481,8 +483,8 @@ int qk_run(const qk_config *cfg, const qk_circuit *c, qk_sv *sv, double *seconds
         if (e != cudaSuccess) rc = cuda_fail(e, "timing");
         else if (seconds) *seconds = ms / 1e3;
     }
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
     if (plan) qk_plan_destroy(plan);
     return rc;
 }
