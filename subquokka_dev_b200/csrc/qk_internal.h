@@ -24,6 +24,7 @@ enum OpKind : int32_t {
     OP_PERM = 7,    // swap bit q[i] with bit q[k+i], i < k = nq/2 (VSWAP_k_k)
     OP_GRAD = 8,    // adjoint sweep: grad[aux] += Im <lambda|G|psi>, G on q[0] = X/Y/Z by m[0] = 1/2/3
     OP_CX = 9,      // flip bit q[1 - aux] where bit q[aux] is set (a U2 that is exactly a CNOT)
+    OP_CDENSE1 = 10,  // 2x2 on q[0]: m[0..7] where bit q[1] is 0, m[8..15] where it is 1 (planner-made)
 };
 
 struct Op {
@@ -48,9 +49,12 @@ inline bool op_is_diagonal(const Op &op) {
 }
 
 // Qubits of an op that a fused pass must hold in registers: q[reg_first(op)
-// .. + reg_count(op)).  None for diagonal ops, the target for OP_CX (its
-// control may be any qubit, as for a diagonal op), all of them otherwise.
-inline int op_reg_count(const Op &op) { return op_is_diagonal(op) ? 0 : op.kind == OP_CX ? 1 : op.nq; }
+// .. + reg_count(op)).  None for diagonal ops, the target for OP_CX and
+// OP_CDENSE1 (the control / condition may be any qubit, as for a diagonal
+// op), all of them otherwise.
+inline int op_reg_count(const Op &op) {
+    return op_is_diagonal(op) ? 0 : (op.kind == OP_CX || op.kind == OP_CDENSE1) ? 1 : op.nq;
+}
 inline int op_reg_first(const Op &op) { return op.kind == OP_CX ? 1 - op.aux : 0; }
 
 }  // namespace qk
@@ -80,6 +84,7 @@ enum TOpKind : uint8_t {
     TOP_PHASE = 4,  // amplitude *= coef[0] where bit(a) = bit(b) = 1 (Z, P, CP; b may be none)
     TOP_GRAD = 5,   // two-state passes: gacc[coef] += Im <lambda|G|psi>, G = X/Y/Z (b = 1/2/3) on slot a
     TOP_CX = 6,     // swap register slot a's pairs where qubit code b is 1 (controlled X)
+    TOP_CG1 = 7,    // dense 2x2 on slot a: coef[0..3] or coef[4..7] by qubit code b (not a register slot)
 };
 
 // Qubit codes of TOP_DIAG / TOP_PHASE: < 0x80 tile-local bit; 0x80 | q global

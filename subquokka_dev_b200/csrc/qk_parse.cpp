@@ -260,6 +260,18 @@ void invert_op(Op &op) {
         std::memcpy(op.m, m, sizeof(double) * 2 * d * d);
         break;
     }
+    case OP_CDENSE1:   // each of the two 2x2 matrices
+        for (int h = 0; h < 2; ++h) {
+            double *a = op.m + 8 * h;
+            const double m01r = a[2], m01i = a[3];
+            a[1] = -a[1];
+            a[7] = -a[7];
+            a[2] = a[4];
+            a[3] = -a[5];
+            a[4] = m01r;
+            a[5] = -m01i;
+        }
+        break;
     case OP_PHASE1: case OP_PHASE2: conj(0); break;
     case OP_DIAG1: conj(0); conj(1); break;
     case OP_DIAG2: for (int k = 0; k < 4; ++k) conj(k); break;

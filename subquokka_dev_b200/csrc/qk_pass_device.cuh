@@ -438,6 +438,22 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             }
             break;
         }
+        case TOP_CG1: {
+            // the condition qubit holds no register slot here, so its value is
+            // the same for all of the thread's amplitudes: one 2x2 of the two
+            const C *m = coef + op.coef + ((bit_set_at(op.b, op.bits[1], 0, base, tb) & 1u) ? 4 : 0);
+            const C m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3];
+            switch (op.a) {
+#define QK_CG1(S)                                                  \
+    case S:                                                        \
+        reg_g1<S>(v, m0, m1, m2, m3);                              \
+        if constexpr (NS == 2) reg_g1<S>(w, m0, m1, m2, m3);       \
+        break;
+            QK_CG1(0) QK_CG1(1) QK_CG1(2) QK_CG1(3) QK_CG1(4)
+#undef QK_CG1
+            }
+            break;
+        }
         case TOP_PHASE: {
             const C ph = coef[op.coef];
             const uint32_t M = bit_set_at(op.a, op.bits[0], 1, base, tb) & bit_set_at(op.b, op.bits[1], 1, base, tb);

@@ -137,6 +137,22 @@ void merge_one_qubit_runs(std::vector<Op> &ops, int n) {
     ops.swap(out);
 }
 
+// 2 x 2 complex products, row-major (re, im) pairs.
+void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]) {   // z = x y
+    for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < 2; ++c) {
+            double re = 0, im = 0;
+            for (int k = 0; k < 2; ++k) {
+                const double xr = x[2 * (2 * r + k)], xi = x[2 * (2 * r + k) + 1];
+                const double yr = y[2 * (2 * k + c)], yi = y[2 * (2 * k + c) + 1];
+                re += xr * yr - xi * yi;
+                im += xr * yi + xi * yr;
+            }
+            z[2 * (2 * r + c)] = re;
+            z[2 * (2 * r + c) + 1] = im;
+        }
+}
+
 // 4 x 4 matrix of a two-qubit op, index b(q[0]) + 2 b(q[1]), row-major (re, im).
 void op_matrix4(const Op &op, double (&m)[32]) {
     std::memset(m, 0, sizeof m);
@@ -160,7 +176,11 @@ void op_matrix4(const Op &op, double (&m)[32]) {
 // ops on other qubits only).  Two dense one-qubit ops and any two-qubit op
 // give a dense 4 x 4 op, which costs the arithmetic of the two 2 x 2 ops it
 // replaces; three diagonal ops give a diagonal one.  Other mixes are left
-// alone, since they would add arithmetic.  On the brick circuits (U3 on
+// alone, since they would add arithmetic; but a diagonal op or a CX with
+// only one qubit's pending op dense takes that op in as OP_CDENSE1 (the
+// 26-qubit HEA forward: 685 -> 375 program ops, 37 -> 30 ms c128; folding
+// one of two pending ops this way instead of both was slower on the brick
+// circuit, 689 against 679 ms).  On the brick circuits (U3 on
 // every qubit, then CZ pairs) this removes two of every three ops: the
 // 30-qubit 20-layer circuit has 407 program ops instead of 941 and, though a
 // dense op needs both qubits in the tile (39 passes instead of 26), runs in
@@ -174,6 +194,47 @@ void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n) {
     for (const Op &op : ops) {
         const bool two = op.nq == 2 && (op.kind == OP_DENSE2 || op.kind == OP_PHASE2 || op.kind == OP_DIAG2 ||
                                         op.kind == OP_SWAP2 || op.kind == OP_CX);
+        // with one qubit's pending op dense (not both), a diagonal op or a CX
+        // takes it in as a one-qubit op conditioned on the other qubit, which
+        // may then lie anywhere, as for the diagonal op itself
+        const bool both = two && last[op.q[0]] >= 0 && last[op.q[1]] >= 0 && out[last[op.q[0]]].kind == OP_DENSE1 &&
+                          out[last[op.q[1]]].kind == OP_DENSE1;
+        if (!both && two && (op.kind == OP_PHASE2 || op.kind == OP_DIAG2 || op.kind == OP_CX)) {
+            int x = -1;   // index in op.q of the target
+            if (op.kind == OP_CX) x = last[op.q[1 - op.aux]] >= 0 && out[last[op.q[1 - op.aux]]].kind == OP_DENSE1 ? 1 - op.aux : -1;
+            else if (last[op.q[0]] >= 0 && out[last[op.q[0]]].kind == OP_DENSE1) x = 0;
+            else if (last[op.q[1]] >= 0 && out[last[op.q[1]]].kind == OP_DENSE1) x = 1;
+            if (x >= 0) {
+                const Op &u = out[last[op.q[x]]];
+                double o4[32];
+                op_matrix4(op, o4);
+                Op f;
+                std::memset(&f, 0, sizeof f);
+                f.kind = OP_CDENSE1;
+                f.nq = 2;
+                f.q[0] = op.q[x];
+                f.q[1] = op.q[1 - x];
+                for (int bc = 0; bc < 2; ++bc) {
+                    // the 2x2 block of o4 on the target for condition value bc
+                    double blk[8], res[8];
+                    for (int rt = 0; rt < 2; ++rt)
+                        for (int ct = 0; ct < 2; ++ct) {
+                            const int r = x == 0 ? rt + 2 * bc : bc + 2 * rt, c = x == 0 ? ct + 2 * bc : bc + 2 * ct;
+                            blk[2 * (2 * rt + ct)] = o4[2 * (4 * r + c)];
+                            blk[2 * (2 * rt + ct) + 1] = o4[2 * (4 * r + c) + 1];
+                        }
+                    double um[8];
+                    as_matrix(u, um);
+                    mat2_mul(blk, um, res);
+                    for (int k = 0; k < 8; ++k) f.m[8 * bc + k] = res[k];
+                }
+                dead[last[op.q[x]]] = 1;
+                last[op.q[0]] = last[op.q[1]] = -1;
+                out.push_back(f);
+                dead.push_back(0);
+                continue;
+            }
+        }
         if (two && last[op.q[0]] >= 0 && last[op.q[1]] >= 0) {
             const Op &u0 = out[last[op.q[0]]], &u1 = out[last[op.q[1]]];
             const bool dense = u0.kind == OP_DENSE1 && u1.kind == OP_DENSE1;
@@ -236,21 +297,6 @@ void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n) {
     ops.swap(kept);
 }
 
-// 2 x 2 complex products, row-major (re, im) pairs.
-void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]) {   // z = x y
-    for (int r = 0; r < 2; ++r)
-        for (int c = 0; c < 2; ++c) {
-            double re = 0, im = 0;
-            for (int k = 0; k < 2; ++k) {
-                const double xr = x[2 * (2 * r + k)], xi = x[2 * (2 * r + k) + 1];
-                const double yr = y[2 * (2 * k + c)], yi = y[2 * (2 * k + c) + 1];
-                re += xr * yr - xi * yi;
-                im += xr * yi + xi * yr;
-            }
-            z[2 * (2 * r + c)] = re;
-            z[2 * (2 * r + c) + 1] = im;
-        }
-}
 
 // Gradient ops of a backward sweep move to the start of their qubit's run of
 // one-qubit ops.  After ops U_1 .. U_k on that qubit (and any ops on other
@@ -385,7 +431,7 @@ size_t program_budget(int dtype, int T, int nstates) {
 size_t op_cost(const Op &op, int dtype) {
     const size_t c = dtype == QK_C128 ? 16 : 8;
     size_t ncoef = 4;
-    if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2) ncoef = 16;
+    if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2 || op.kind == OP_CDENSE1) ncoef = 16;
     else if (op.kind == OP_PHASE1 || op.kind == OP_PHASE2) ncoef = 1;
     else if (op.kind == OP_CX) ncoef = 0;
     else if (op.kind == OP_GRAD) {
@@ -575,6 +621,34 @@ struct PassBuilder {
             t.a = (uint8_t)slot(op.q[1 - op.aux]);
             t.b = code(op.q[op.aux], local);
             break;
+        case OP_CDENSE1: {
+            // condition in a register slot here: the block-diagonal 4 x 4
+            // (index b(target) + 2 b(condition)); otherwise the condition is
+            // the same for all of a thread's amplitudes and TOP_CG1 picks one
+            // of the two 2x2 matrices
+            if (local[op.q[1]] >= 0 && slot(op.q[1]) < (int)Q.size()) {
+                Op d;
+                std::memset(&d, 0, sizeof d);
+                d.kind = OP_DENSE2;
+                d.nq = 2;
+                d.q[0] = op.q[0];
+                d.q[1] = op.q[1];
+                for (int rc = 0; rc < 2; ++rc)
+                    for (int rt = 0; rt < 2; ++rt)
+                        for (int ct = 0; ct < 2; ++ct) {
+                            const int k = 4 * (rt + 2 * rc) + (ct + 2 * rc);
+                            d.m[2 * k] = op.m[8 * rc + 2 * (2 * rt + ct)];
+                            d.m[2 * k + 1] = op.m[8 * rc + 2 * (2 * rt + ct) + 1];
+                        }
+                emit(d, local, Q);
+                return;
+            }
+            t.kind = TOP_CG1;
+            t.a = (uint8_t)slot(op.q[0]);
+            t.b = code(op.q[1], local);
+            for (int k = 0; k < 8; ++k) push_c(plan, op.m[2 * k], op.m[2 * k + 1]);
+            break;
+        }
         case OP_PHASE1:
             t.kind = TOP_PHASE;
             t.a = code(op.q[0], local);
@@ -605,13 +679,13 @@ struct PassBuilder {
         // condition qubits of DIAG / PHASE (a, b) and CX (b): their register
         // slot in bits[0] / bits[1] (kNoSlot when not register-resident), so
         // that the kernel need not search the current mapping
-        if (t.kind == TOP_DIAG || t.kind == TOP_PHASE || t.kind == TOP_CX) {
+        if (t.kind == TOP_DIAG || t.kind == TOP_PHASE || t.kind == TOP_CX || t.kind == TOP_CG1) {
             auto slot_of = [&](uint8_t c) -> uint8_t {
                 if (c == kNoQubit || (c & kOuterFlag)) return kNoSlot;
                 const auto it = std::find(Q.begin(), Q.end(), (int)c);
                 return it == Q.end() ? kNoSlot : (uint8_t)(it - Q.begin());
             };
-            t.bits[0] = t.kind == TOP_CX ? kNoSlot : slot_of(t.a);
+            t.bits[0] = (t.kind == TOP_CX || t.kind == TOP_CG1) ? kNoSlot : slot_of(t.a);
             t.bits[1] = slot_of(t.b);
         }
         plan.ops.push_back(t);
