@@ -23,6 +23,22 @@ def test_diagonal_gates_join_any_pass():
     assert Plan(c, n, "c128").stats()[0] == 1
 
 
+def test_program_op_reductions():
+    # consecutive one-qubit ops multiply into one, two pending dense ops fold
+    # into the two-qubit op after them, one pending dense op folds into a
+    # diagonal op or CX as a conditioned 2x2: the 26-qubit HEA forward pass
+    # (924 gates) and the 30-qubit brick circuit (890 gates) need far fewer
+    # program ops than gates
+    from subquokka_dev_b200.torch_shim import hea_template
+    pc = hea_template(26, 12)
+    c, _ = pc.bind(np.random.default_rng(26).uniform(-np.pi, np.pi, pc.nparams))
+    assert c.ngates == 924
+    passes, ops, _ = Plan(c, 26, "c128").stats()
+    assert ops <= 400 and passes <= 30
+    brick = circuits.random_u3_cz(30, 20, 2030)
+    assert Plan(brick, 30, "c64").stats()[1] <= 420
+
+
 def test_vswap_is_a_relabelling():
     # H 0, VSWAP, H 1 = H on stored bits 0 and 15 in one pass, then one
     # permutation pass that brings the state into the circuit's layout
