@@ -138,6 +138,16 @@ struct PlanOptions {
 int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, HostPlan &plan);
 // One permutation pass (an OP_PERM of 1 to 6 bit pairs), with no program.
 int build_perm_plan(const Op &op, int n, const PlanOptions &o, HostPlan &plan);
+// Op-list rewrites before planning (qk_rewrite.cpp).
+bool one_qubit(const Op &op);
+void as_matrix(const Op &op, double (&m)[8]);
+void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]);
+void asap_order(std::vector<Op> &ops, int n);
+void merge_one_qubit_runs(std::vector<Op> &ops, int n);
+void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n);
+void hoist_gradients(std::vector<Op> &ops, int n);
+void pair_gradients(std::vector<Op> &ops);
+void relabel_perms(std::vector<Op> &ops, int n, int L, int max_bits, int max_pairs, bool swaps);
 // Plan of a subcircuit file (the subcircuit path): the gates of all groups
 // as one gate list, VSWAPs as renamings of the qubits after them.
 int build_group_plan(const qk_gate *gates, const int32_t *sizes, size_t ngroups, int n, const PlanOptions &o,
