@@ -1,0 +1,285 @@
+// CPU check of the fused-pass planner (subquokka_dev_b200/csrc/qk_plan.cpp).
+//
+// The pass programs of a HostPlan are run by an emulator written from their
+// definitions in qk_internal.h: a pass gathers every tile (2^T amplitudes
+// whose index bits are the pass's state bits bpos) and runs its program on
+// it; register slot s stands for tile bit Q[s] as the last TOP_REMAP set it;
+// condition codes name a tile bit, a state bit outside the tile (constant
+// over the tile) or none.  The thread and register layout of the CUDA
+// interpreter plays no part: what is checked is the plan itself (pass
+// choice, slots, condition codes, coefficient order, gradient slots,
+// permutation passes).  Random circuits (every MEM gate, random U1/U2,
+// CNOT-shaped U2s, VSWAPs) with small tiles, so that each plan has many
+// passes and re-mappings:
+// - forward plans (build_plan, both dtypes' budgets) against the dense
+//   simulation of the gate list;
+// - adjoint plans (build_adjoint_plan) against the direct backward sweep:
+//   the inverse gates from last to first on psi and lambda, the gradient of
+//   each trainable gate taken just before its inverse.
+// States agree within 1e-12; gradients within 1e-12, or 1e-9 for circuits
+// with H (the reference's H constant is 1.1e-11 off unitary, and gradient
+// ops move past gates on other qubits).  Exit status 0 on success.
+#include "dense_sim.h"
+
+using namespace dense_sim;
+using qk::HostPlan;
+using qk::PassDesc;
+using qk::TOp;
+
+namespace {
+
+int bit_of(uint8_t code, uint64_t j, uint64_t base) {
+    if (code == qk::kNoQubit) return -1;
+    if (code & qk::kOuterFlag) return (int)((base >> (code & 0x7F)) & 1);
+    return (int)((j >> code) & 1);
+}
+
+// run every pass of hp on psi (and lam when two-state); gradients into g
+void emulate(const HostPlan &hp, State &psi, State *lam, std::vector<double> &g) {
+    const int n = hp.n;
+    for (const PassDesc &d : hp.passes) {
+        State *states[2] = {&psi, lam};
+        if (d.perm == 2) {   // flat permutation: state bits perm_a[i] <-> perm_b[i]
+            Op p;
+            std::memset(&p, 0, sizeof p);
+            p.kind = qk::OP_PERM;
+            p.nq = 2 * d.nperm;
+            for (int i = 0; i < d.nperm; ++i) {
+                p.q[i] = d.perm_a[i];
+                p.q[d.nperm + i] = d.perm_b[i];
+            }
+            std::vector<int> qs;
+            const auto m = matrix_of(p, qs);
+            for (State *s : states)
+                if (s) apply_matrix(*s, n, qs, m);
+            continue;
+        }
+        const int T = d.T;
+        const uint64_t tn = 1ull << T;
+        std::vector<int> outer;
+        std::vector<char> in_tile(n, 0);
+        for (int k = 0; k < T; ++k) in_tile[d.bpos[k]] = 1;
+        for (int q = 0; q < n; ++q)
+            if (!in_tile[q]) outer.push_back(q);
+        auto addr = [&](uint64_t base, uint64_t j) {
+            uint64_t a = base;
+            for (int k = 0; k < T; ++k)
+                if ((j >> k) & 1) a |= 1ull << d.bpos[k];
+            return a;
+        };
+        for (uint64_t t = 0; t < (1ull << outer.size()); ++t) {
+            uint64_t base = 0;
+            for (size_t k = 0; k < outer.size(); ++k)
+                if ((t >> k) & 1) base |= 1ull << outer[k];
+            std::vector<cd> x[2];
+            for (int si = 0; si < 2; ++si)
+                if (states[si]) {
+                    x[si].resize(tn);
+                    for (uint64_t j = 0; j < tn; ++j) x[si][j] = (*states[si])[addr(base, j)];
+                }
+            if (d.perm == 1) {   // tile-local bit pairs swapped on store
+                for (int si = 0; si < 2; ++si)
+                    if (states[si])
+                        for (uint64_t j = 0; j < tn; ++j) {
+                            uint64_t r = j;
+                            for (int i = 0; i < d.nperm; ++i) {
+                                const uint64_t a = (j >> d.perm_a[i]) & 1, b = (j >> d.perm_b[i]) & 1;
+                                r = (r & ~(1ull << d.perm_a[i]) & ~(1ull << d.perm_b[i])) | (b << d.perm_a[i]) |
+                                    (a << d.perm_b[i]);
+                            }
+                            (*states[si])[addr(base, r)] = x[si][j];
+                        }
+                continue;
+            }
+            std::vector<int> Q;
+            auto coef = [&](const TOp &op, int k) {
+                const size_t i = (size_t)(d.coef0 + op.coef + k);
+                return cd(hp.coef[2 * i], hp.coef[2 * i + 1]);
+            };
+            auto pairs = [&](int tb, auto &&f) {
+                for (uint64_t j = 0; j < tn; ++j)
+                    if (!((j >> tb) & 1)) f(j, j | (1ull << tb));
+            };
+            for (int pi = d.prog0; pi < d.prog0 + d.nprog; ++pi) {
+                const TOp &op = hp.ops[pi];
+                switch (op.kind) {
+                case qk::TOP_REMAP:
+                    Q.assign(op.bits, op.bits + op.nbits);
+                    break;
+                case qk::TOP_G1:
+                case qk::TOP_CG1:
+                case qk::TOP_CX:
+                    for (int si = 0; si < 2; ++si)
+                        if (states[si])
+                            pairs(Q.at(op.a), [&](uint64_t j0, uint64_t j1) {
+                                const cd a = x[si][j0], b = x[si][j1];
+                                if (op.kind == qk::TOP_CX) {
+                                    if (bit_of(op.b, j0, base) == 1) std::swap(x[si][j0], x[si][j1]);
+                                    return;
+                                }
+                                const int off = op.kind == qk::TOP_CG1 && bit_of(op.b, j0, base) == 1 ? 4 : 0;
+                                x[si][j0] = coef(op, off) * a + coef(op, off + 1) * b;
+                                x[si][j1] = coef(op, off + 2) * a + coef(op, off + 3) * b;
+                            });
+                    break;
+                case qk::TOP_G2: {
+                    const int ta = Q.at(op.a), tb = Q.at(op.b);
+                    for (int si = 0; si < 2; ++si)
+                        if (states[si])
+                            for (uint64_t j = 0; j < tn; ++j) {
+                                if (((j >> ta) & 1) || ((j >> tb) & 1)) continue;
+                                const uint64_t idx[4] = {j, j | (1ull << ta), j | (1ull << tb),
+                                                         j | (1ull << ta) | (1ull << tb)};
+                                cd in[4], out[4];
+                                for (int k = 0; k < 4; ++k) in[k] = x[si][idx[k]];
+                                for (int r = 0; r < 4; ++r) {
+                                    out[r] = 0;
+                                    for (int k = 0; k < 4; ++k) out[r] += coef(op, 4 * r + k) * in[k];
+                                }
+                                for (int k = 0; k < 4; ++k) x[si][idx[k]] = out[k];
+                            }
+                    break;
+                }
+                case qk::TOP_DIAG:
+                case qk::TOP_PHASE:
+                    for (int si = 0; si < 2; ++si)
+                        if (states[si])
+                            for (uint64_t j = 0; j < tn; ++j) {
+                                const int ba = bit_of(op.a, j, base), bb = bit_of(op.b, j, base);
+                                if (op.kind == qk::TOP_DIAG)
+                                    x[si][j] *= coef(op, (ba < 0 ? 0 : ba) + 2 * (bb < 0 ? 0 : bb));
+                                else if (ba != 0 && bb != 0)
+                                    x[si][j] *= coef(op, 0);
+                            }
+                    break;
+                case qk::TOP_GRAD: {
+                    const int gen = op.b;
+                    const int tb = Q.at(op.a);
+                    for (int w = 0; w < (gen == 5 ? 2 : 1); ++w) {
+                        double a = gen == 1, b = gen == 2, cz = gen == 3;
+                        if (gen >= 4) {
+                            a = coef(op, 2 * w).real();
+                            b = coef(op, 2 * w).imag();
+                            cz = coef(op, 2 * w + 1).real();
+                        }
+                        const int slot = w ? (op.bits[2] | (op.bits[3] << 8)) : (op.bits[0] | (op.bits[1] << 8));
+                        const int param = hp.grad_params.at((size_t)(d.grad0 + slot));
+                        const cd g00 = cz, g01 = cd(a, -b), g10 = cd(a, b), g11 = -cz;
+                        double s = 0;
+                        pairs(tb, [&](uint64_t j0, uint64_t j1) {
+                            const cd p0 = x[0][j0], p1 = x[0][j1], l0 = x[1][j0], l1 = x[1][j1];
+                            s += (std::conj(l0) * (g00 * p0 + g01 * p1) + std::conj(l1) * (g10 * p0 + g11 * p1)).imag();
+                        });
+                        g.at(param) += s;
+                    }
+                    break;
+                }
+                default:
+                    std::fprintf(stderr, "unknown program op %d\n", op.kind);
+                    std::exit(2);
+                }
+            }
+            for (int si = 0; si < 2; ++si)
+                if (states[si])
+                    for (uint64_t j = 0; j < tn; ++j) (*states[si])[addr(base, j)] = x[si][j];
+        }
+    }
+}
+
+}  // namespace
+
+int main() {
+    int bad = 0, plans = 0;
+    for (int seed = 0; seed < 80; ++seed) {
+        const bool with_h = seed % 2;
+        Gen G{std::mt19937_64(1000 + seed), 6 + seed % 3, with_h};
+        const int n = G.n;
+        const int T = 4 + seed % 3, r = 2 + (seed / 3) % 2;
+        qk::PlanOptions o{seed % 4 < 2 ? QK_C128 : QK_C64, T, r};
+        // forward
+        std::vector<qk_gate> gates;
+        for (int i = 0; i < 70; ++i) {
+            if (i % 23 == 7) {
+                qk_gate v;
+                std::memset(&v, 0, sizeof v);
+                const Op p = G.vswap();
+                v.kind = QK_GATE_VSWAP;
+                v.nq = 4;
+                for (int k = 0; k < 4; ++k) v.q[k] = p.q[k];
+                gates.push_back(v);
+            } else {
+                gates.push_back(G.gate());
+            }
+        }
+        HostPlan hp;
+        if (qk::build_plan(gates.data(), gates.size(), n, o, hp)) {
+            std::printf("seed %d: build_plan failed: %s\n", seed, qk_last_error());
+            ++bad;
+            continue;
+        }
+        ++plans;
+        State ref = G.state(), got = ref, dummy = ref;
+        std::vector<double> none(1, 0);
+        for (const qk_gate &g : gates) {
+            std::vector<int> qs;
+            const Op op = lower(g);
+            const auto m = matrix_of(op, qs);
+            apply_matrix(ref, n, qs, m);
+        }
+        emulate(hp, got, nullptr, none);
+        const double df = max_diff(ref, got);
+        if (df > 1e-12) {
+            std::printf("forward seed %d (n %d, T %d, r %d): max |d amp| %.3g, %zu passes\n", seed, n, T, r, df,
+                        hp.passes.size());
+            ++bad;
+        }
+        // adjoint: trainable RX / RY / RZ, some sharing a parameter
+        std::vector<qk_gate> circ;
+        std::vector<int32_t> pidx;
+        int np = 0;
+        for (int i = 0; i < 70; ++i) {
+            const qk_gate g = G.gate();
+            circ.push_back(g);
+            const bool rot = g.kind == QK_GATE_RX || g.kind == QK_GATE_RY || g.kind == QK_GATE_RZ;
+            pidx.push_back(rot ? (np > 2 && G.rng() % 4 == 0 ? (int)(G.rng() % np) : np++) : -1);
+        }
+        qk::PlanOptions ao{o.dtype, std::min(T, 6), 2 + seed % 2};
+        HostPlan ap;
+        if (qk::build_adjoint_plan(circ.data(), circ.size(), pidx.data(), n, ao, ap)) {
+            std::printf("seed %d: build_adjoint_plan failed: %s\n", seed, qk_last_error());
+            ++bad;
+            continue;
+        }
+        ++plans;
+        std::vector<Op> back;
+        for (size_t i = circ.size(); i-- > 0;) {
+            Op op = lower(circ[i]);
+            if (pidx[i] >= 0) {
+                Op gr;
+                std::memset(&gr, 0, sizeof gr);
+                gr.kind = qk::OP_GRAD;
+                gr.nq = 1;
+                gr.q[0] = op.q[0];
+                gr.m[0] = circ[i].kind == QK_GATE_RX ? 1 : circ[i].kind == QK_GATE_RY ? 2 : 3;
+                gr.aux = pidx[i];
+                back.push_back(gr);
+            }
+            qk::invert_op(op);
+            back.push_back(op);
+        }
+        State psi = G.state(), lam = G.state(), psi2 = psi, lam2 = lam;
+        std::vector<double> g0(np + 1, 0), g1(np + 1, 0);
+        run(back, n, psi, lam, g0);
+        emulate(ap, psi2, &lam2, g1);
+        double dg = 0;
+        for (int k = 0; k <= np; ++k) dg = std::max(dg, std::fabs(g0[k] - g1[k]));
+        const double ds = std::max(max_diff(psi, psi2), max_diff(lam, lam2));
+        if (dg > (with_h ? 1e-9 : 1e-12) || ds > 1e-12) {
+            std::printf("adjoint seed %d (n %d, T %d): max |d grad| %.3g, max |d amp| %.3g, %zu passes\n", seed, n,
+                        ao.tile_bits, dg, ds, ap.passes.size());
+            ++bad;
+        }
+    }
+    std::printf("%d plans, %s\n", plans, bad ? "FAIL" : "ok");
+    return bad ? 1 : 0;
+}

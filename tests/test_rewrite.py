@@ -1,8 +1,11 @@
-"""The op-list rewrites the planners apply before compiling pass programs
-(one-qubit merges, folds into two-qubit and conditioned ops, gradient
-hoisting and pairing, ASAP order, VSWAP renaming) keep the states and
-gradients a list computes: tests/rewrite_check.cpp runs random lists and
-their rewritten forms on small dense states on the CPU."""
+"""CPU checks of the planner, built from the host sources with g++:
+- tests/rewrite_check.cpp: the op-list rewrites the planners apply before
+  compiling pass programs (one-qubit merges, folds into two-qubit and
+  conditioned ops, gradient hoisting and pairing, ASAP order, VSWAP
+  renaming) keep the states and gradients a list computes;
+- tests/plan_check.cpp: forward and adjoint fused plans, run by an emulator
+  of the pass programs, give the states and gradients of the dense
+  simulation of their gate lists."""
 import os
 import shutil
 import subprocess
@@ -13,13 +16,22 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "subquokka_dev_b200", "csrc")
 
 
-@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ absent")
-def test_rewrites_keep_states_and_gradients(tmp_path):
-    exe = tmp_path / "rewrite_check"
-    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           os.path.join(ROOT, "tests", "rewrite_check.cpp"), os.path.join(CSRC, "qk_rewrite.cpp"),
-           os.path.join(CSRC, "qk_parse.cpp"), "-o", str(exe)]
+def build_and_run(tmp_path, main, sources):
+    exe = tmp_path / main.replace(".cpp", "")
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I",
+           os.path.join(ROOT, "tests"), os.path.join(ROOT, "tests", main)]
+    cmd += [os.path.join(CSRC, f) for f in sources] + ["-o", str(exe)]
     build = subprocess.run(cmd, capture_output=True, text=True)
     assert build.returncode == 0, build.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ absent")
+def test_rewrites_keep_states_and_gradients(tmp_path):
+    build_and_run(tmp_path, "rewrite_check.cpp", ["qk_rewrite.cpp", "qk_parse.cpp"])
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ absent")
+def test_plans_compute_the_circuit(tmp_path):
+    build_and_run(tmp_path, "plan_check.cpp", ["qk_plan.cpp", "qk_rewrite.cpp", "qk_parse.cpp"])
