@@ -17,13 +17,18 @@ CSRC = os.path.join(ROOT, "subquokka_dev_b200", "csrc")
 
 
 def build_and_run(tmp_path, main, sources):
+    # built with AddressSanitizer and UndefinedBehaviorSanitizer: the host
+    # planner code also runs free of memory errors, leaks and undefined
+    # behaviour on these inputs
     exe = tmp_path / main.replace(".cpp", "")
-    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I",
-           os.path.join(ROOT, "tests"), os.path.join(ROOT, "tests", main)]
+    cmd = ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", os.path.join(ROOT, "tests"),
+           os.path.join(ROOT, "tests", main)]
     cmd += [os.path.join(CSRC, f) for f in sources] + ["-o", str(exe)]
     build = subprocess.run(cmd, capture_output=True, text=True)
     assert build.returncode == 0, build.stderr
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    env = dict(os.environ, UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1", ASAN_OPTIONS="detect_leaks=1")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300, env=env)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
 
 
