@@ -13,6 +13,8 @@
 // passes and re-mappings:
 // - forward plans (build_plan, both dtypes' budgets) against the dense
 //   simulation of the gate list;
+// - tensor-core dense-block plans (build_dense_blocks, widths 5 and 6)
+//   against the same dense simulation;
 // - adjoint plans (build_adjoint_plan) against the direct backward sweep:
 //   the inverse gates from last to first on psi and lambda, the gradient of
 //   each trainable gate taken just before its inverse.
@@ -232,6 +234,40 @@ int main() {
             std::printf("forward seed %d (n %d, T %d, r %d): max |d amp| %.3g, %zu passes\n", seed, n, T, r, df,
                         hp.passes.size());
             ++bad;
+        }
+        // tensor-core dense blocks (64 x 64 unitaries on six qubits, block
+        // index bit b = qubit q[b]; permutation blocks for the restore)
+        for (int width : {5, 6}) {
+            std::vector<qk::DenseBlock> blocks;
+            if (qk::build_dense_blocks(gates.data(), gates.size(), n, width, blocks)) {
+                std::printf("seed %d: build_dense_blocks failed: %s\n", seed, qk_last_error());
+                ++bad;
+                continue;
+            }
+            ++plans;
+            State want = G.state(), have = want;
+            for (const qk_gate &g : gates) {
+                std::vector<int> qs;
+                const auto m = matrix_of(lower(g), qs);
+                apply_matrix(want, n, qs, m);
+            }
+            for (const qk::DenseBlock &b : blocks) {
+                std::vector<int> qs;
+                if (b.perm) {
+                    const auto m = matrix_of(b.perm_op, qs);
+                    apply_matrix(have, n, qs, m);
+                    continue;
+                }
+                qs.assign(b.q, b.q + qk::kDenseQubits);
+                std::vector<cd> u((size_t)qk::kDenseDim * qk::kDenseDim);
+                for (size_t k = 0; k < u.size(); ++k) u[k] = cd(b.u[2 * k], b.u[2 * k + 1]);
+                apply_matrix(have, n, qs, u);
+            }
+            const double dd = max_diff(want, have);
+            if (dd > 1e-12) {
+                std::printf("dense seed %d width %d: max |d amp| %.3g, %zu blocks\n", seed, width, dd, blocks.size());
+                ++bad;
+            }
         }
         // adjoint: trainable RX / RY / RZ, some sharing a parameter
         std::vector<qk_gate> circ;
