@@ -109,7 +109,7 @@ class Circuit:
                 lines.append(str(n))
                 lines += [gate_line(self.gates[k + j]) for j in range(n)]
                 k += n
-        return "\n".join(lines) + "\n"
+        return "\n".join(lines) + "\n" if lines else ""
 
 
 def chunk_groups(circuit: Circuit, n: int, chunk_qbit: int = 12) -> Circuit:

@@ -102,6 +102,19 @@ def test_qft30_vswap_count():
     assert sum(1 for k, _ in kinds[:last_compute] if k == VSWAP) < 42
 
 
+def test_empty_and_small_circuits():
+    empty = chunk_groups(Circuit([]), 5, 2)
+    assert empty.ngates == 0 and empty.to_text(True) == ""
+    assert Circuit.parse(empty.to_text(True), 1, 5).ngates == 0
+    one = chunk_groups(Circuit([make_gate("H", [0]), make_gate("RX", [0], 0.3)]), 1, 1)
+    assert one.ngates == 2 and one.ngroups == 1
+    # chunk = whole state: no VSWAP, the final SWAPs as in-chunk SWAP gates
+    full = chunk_groups(circuits.qft(6), 6, 6)
+    check_contract(full, 6)
+    init = circuits.random_state(6, 3)
+    assert np.abs(oracle.apply_circuit(init, 6, full) - oracle.apply_circuit(init, 6, circuits.qft(6))).max() <= 1e-12
+
+
 def test_chunk_groups_errors():
     circ = Circuit([make_gate("CP", [0, 1], 0.1)])
     for n, c in ((0, 1), (4, 0), (4, 5)):
