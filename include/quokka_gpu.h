@@ -378,9 +378,12 @@ void qk_batch_destroy(qk_batch *b);
  * programs go to a fixed __device__ array of QK_NOALLOC_SCRATCH_BYTES that
  * every GPU loading the library holds until exit; a circuit whose programs do
  * not fit returns QK_ERR_ARG.  The first call on a device looks up that
- * array's address (make it before any stream capture on the device).  Every
- * call shares the array and overwrites it: calls that overlap on the GPU
- * (unordered streams) race; calls on one stream are safe. */
+ * array's address (make it before any stream capture on the device) and keeps
+ * it, so the library must not be used across a cudaDeviceReset.  Every call
+ * shares the array and overwrites it: calls that overlap on the GPU
+ * (unordered streams) race; calls on one stream are safe.  The programs are
+ * copied from host memory the call frees, so it waits for those copies before
+ * returning, and a call on a stream under capture returns QK_ERR_UNSUPPORTED. */
 int qk_apply_fused_noalloc(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n, void *cuda_stream);
 
 /* Run a parsed circuit the way Simulator::run does (src/simulator.cpp:671-706):

@@ -19,19 +19,27 @@ import numpy as np
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_DRIVER = os.path.join(ORACLE_DIR, "_ref", "quokka_ref")
-REF_SOURCE = "/root/reference"
+# the reference checkout whose sources `make ref` compiles; only set where
+# those sources exist (the build and test harnesses pass it in)
+REF_SOURCE = os.environ.get("QUOKKA_REFERENCE_DIR", "")
 
 _lib = None
 
 
-def build(with_reference: bool | None = None) -> None:
-    """Compile the C restatement and, when the reference sources are present,
-    the reference itself (oracle/_ref)."""
+def have_reference_source(ref_dir: str | None = None) -> bool:
+    d = REF_SOURCE if ref_dir is None else ref_dir
+    return bool(d) and os.path.isdir(os.path.join(d, "src"))
+
+
+def build(with_reference: bool | None = None, ref_dir: str | None = None) -> None:
+    """Compile the C restatement and, when the reference sources are present
+    (ref_dir, else $QUOKKA_REFERENCE_DIR), the reference itself (oracle/_ref)."""
+    d = REF_SOURCE if ref_dir is None else ref_dir
     subprocess.run(["make", "-C", ORACLE_DIR], check=True)
     if with_reference is None:
-        with_reference = os.path.isdir(os.path.join(REF_SOURCE, "src"))
+        with_reference = have_reference_source(d)
     if with_reference:
-        subprocess.run(["make", "-C", ORACLE_DIR, "ref", "-j8", f"REF={REF_SOURCE}"], check=True)
+        subprocess.run(["make", "-C", ORACLE_DIR, "ref", "-j8", f"REF={d}"], check=True)
 
 
 def load():

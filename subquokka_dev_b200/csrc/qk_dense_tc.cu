@@ -136,8 +136,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
     extern __shared__ __align__(1024) unsigned char sm[];
     // full[b]: buffer b converted (one arrival per data warp); mma[b]: the
     // contraction of buffer b done (tcgen05.commit); empty[b]: accumulator b
-    // drained (one arrival per data warp)
-    __shared__ __align__(8) uint64_t full[2], mma[2], empty[2];
+    // drained (one arrival per data warp); fin: every MMA the issuer ever
+    // issued has completed (its last tcgen05.commit, made on every exit path)
+    __shared__ __align__(8) uint64_t full[2], mma[2], empty[2], fin;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int bad_s;
     const PassDesc &d = dd.p;
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&mma[b])), "r"(1) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&empty[b])), "r"(kTcDataWarps) : "memory");
         }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&fin)), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (issuer) {
@@ -247,6 +249,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  s_u32(&mma[b]))
                              : "memory");
+            }
+            // Teardown invariant: the TMEM is released only after every MMA
+            // issued above has completed.  On the normal path the data warps
+            // have already waited for the last contraction; on a timeout they
+            // stop early, so MMAs of one or two supertiles may still be in
+            // flight.  tcgen05.commit tracks all earlier tcgen05 operations of
+            // this thread, so one more commit on `fin` arrives only after all
+            // of them; the wait is bounded like every other, and a wait that
+            // runs out is reported (error 3) before the dealloc.
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             s_u32(&fin))
+                         : "memory");
+            if (!tc_wait(&fin, 0)) {
+                bad_s = 1;
+                atomicExch(err, 3);
             }
         }
         __syncwarp();   // the issuer warp reaches the final barrier converged
@@ -423,7 +440,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (bad_s && tid == 0) atomicExch(err, 1);
+    if (bad_s && tid == 0) atomicCAS(err, 0, 1);   // keeps a more specific code (3) set above
     if (issuer) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
 }
 

@@ -12,12 +12,22 @@
 //
 // Set-up: the first call on a device asks the runtime for the array's device
 // address (cudaGetSymbolAddress, with that device current) and caches it;
-// make that first call before any stream capture on the device.  Every later
-// call on any stream shares the one array, and each call overwrites it with
-// its own programs: calls that overlap on the GPU (different streams, no
-// ordering between them) race on it.  Calls on one stream are ordered and
-// safe.  Nothing in the array needs to start at zero: every byte a pass reads
-// is written by the same call first.
+// make that first call before any stream capture on the device.  The cached
+// address belongs to the module the runtime loaded for that device, so the
+// library must not be used across a cudaDeviceReset (the module, and with it
+// the array, may come back at another address).  Every later call on any
+// stream shares the one array, and each call overwrites it with its own
+// programs: calls that overlap on the GPU (different streams, no ordering
+// between them) race on it.  Calls on one stream are ordered and safe.
+// Nothing in the array needs to start at zero: every byte a pass reads is
+// written by the same call first.
+//
+// The programs are copied from host vectors that this call owns and frees on
+// return, so the call waits for its copies to finish (cudaStreamSynchronize)
+// before it returns -- the same rule as every other upload from a host
+// temporary in this library.  A stream that is being captured cannot be
+// synchronised and a captured copy would read freed memory at replay, so a
+// call on a capturing stream is refused with QK_ERR_UNSUPPORTED.
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -67,6 +77,14 @@ extern "C" int qk_apply_fused_noalloc(void *state, int nqubits, int dtype, const
     if (!state || (!gates && n)) return fail(QK_ERR_ARG, "null argument");
     if (nqubits < 1 || nqubits > 36) return fail(QK_ERR_ARG, "nqubits must be in [1, 36], got %d", nqubits);
     if (dtype != QK_C128 && dtype != QK_C64) return fail(QK_ERR_ARG, "unknown dtype %d", dtype);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(st, &cap);
+    if (ce != cudaSuccess) return fail(QK_ERR_CUDA, "cudaStreamIsCapturing: %s", cudaGetErrorString(ce));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(QK_ERR_UNSUPPORTED,
+                    "qk_apply_fused_noalloc copies its programs from host memory it frees on return and waits for "
+                    "them, which a stream under capture cannot do");
     HostPlan hp;
     int rc = build_plan(gates, n, nqubits, default_plan_options(dtype, nqubits), hp);
     if (rc) return rc;
@@ -81,20 +99,20 @@ extern "C" int qk_apply_fused_noalloc(void *state, int nqubits, int dtype, const
     void *base = nullptr;
     rc = scratch_address(&base);
     if (rc) return rc;
-    cudaStream_t st = (cudaStream_t)cuda_stream;
     unsigned char *b = static_cast<unsigned char *>(base);
+    std::vector<float> f;   // complex64 coefficients; must outlive the copy
     cudaError_t e = cudaSuccess;
     if (!hp.ops.empty()) e = cudaMemcpyAsync(b, hp.ops.data(), hp.ops.size() * sizeof(TOp), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && ncoef) {
-        // pageable host -> device copies return once the source is staged, so
-        // the host vectors may go away when this function returns
         if (dtype == QK_C128) {
             e = cudaMemcpyAsync(b + ops_bytes, hp.coef.data(), coef_bytes, cudaMemcpyHostToDevice, st);
         } else {
-            std::vector<float> f(hp.coef.begin(), hp.coef.end());
+            f.assign(hp.coef.begin(), hp.coef.end());
             e = cudaMemcpyAsync(b + ops_bytes, f.data(), coef_bytes, cudaMemcpyHostToDevice, st);
         }
     }
+    // hp and f are freed on return: the copies finish first
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(QK_ERR_CUDA, "copy to scratch: %s", cudaGetErrorString(e));
     return run_plan_at(state, dtype, hp, reinterpret_cast<const TOp *>(b), b + ops_bytes, st);
 }

@@ -255,16 +255,21 @@ static int upload_plan(const HostPlan &hp, int dtype, DevPlan &dp, cudaStream_t 
                             cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return cuda_err(e, "upload plan gradient slots");
     }
+    std::vector<float> f;   // complex64 coefficients; must outlive the copy
     if (nc) {
         if (dtype == QK_C128) {
             e = cudaMemcpyAsync(dp.coef, hp.coef.data(), nc * sizeof(double2), cudaMemcpyHostToDevice, st);
         } else {
-            std::vector<float> f(hp.coef.begin(), hp.coef.end());
+            f.assign(hp.coef.begin(), hp.coef.end());
             e = cudaMemcpyAsync(dp.coef, f.data(), nc * sizeof(float2), cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // f is a temporary
         }
         if (e != cudaSuccess) return cuda_err(e, "upload plan coefficients");
     }
+    // One rule for every upload from host memory in this library: a copy whose
+    // source the caller may free (f here; hp itself when the plan is a
+    // temporary, as for subcircuit files) has finished before the call returns.
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_err(e, "upload plan");
     return QK_OK;
 }
 
@@ -490,6 +495,8 @@ int qk_plan_apply(qk_sv *sv, qk_plan *p) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_err(e, "dense blocks");
         if (herr == 2) return fail(QK_ERR_CUDA, "tensor-core pass: shared memory not 1024-byte aligned");
+        if (herr == 3)
+            return fail(QK_ERR_CUDA, "a tensor-core pass gave up waiting for its last MMAs before releasing TMEM");
         if (herr) return fail(QK_ERR_CUDA, "a tensor-core pass gave up waiting for its contraction");
         return QK_OK;
     }

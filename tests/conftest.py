@@ -7,6 +7,9 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
+# the test harness's default location of the reference checkout (tests that
+# compile against its sources skip where it is absent, e.g. on the GPU box)
+os.environ.setdefault("QUOKKA_REFERENCE_DIR", "/root/reference")
 
 
 def pytest_configure(config):

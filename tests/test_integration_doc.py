@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 OBJ = os.path.join(ROOT, "oracle", "_ref", "obj")
 
 pytestmark = pytest.mark.skipif(
-    shutil.which("g++") is None or not os.path.isdir(os.path.join(oracle.REF_SOURCE, "src")) or not os.path.isdir(OBJ),
+    shutil.which("g++") is None or not oracle.have_reference_source() or not os.path.isdir(OBJ),
     reason="reference sources or their build (oracle/_ref) absent")
 
 
