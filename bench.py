@@ -53,10 +53,14 @@ def parse_args():
 
 
 def config_dict(args, world):
-    return {"workload": f"random circuit, {args.qubits} qubits, {args.layers} layers (U3 on every qubit + brick CZ), "
+    n = args.qubits
+    return {"workload": f"random circuit, {n} qubits, {args.layers} layers (U3 on every qubit + brick CZ), "
                         "complex128, per-gate path",
-            "qubits": args.qubits, "layers": args.layers, "seed": SEED, "state_bytes": 16 << args.qubits,
-            "l2": "inputs larger than L2 (state >> 126 MB)", "parallelism": f"replicas x{world}"}
+            "qubits": n, "layers": args.layers, "seed": SEED, "state_bytes": 16 << n,
+            "l2": "inputs larger than L2 (state >> 126 MB)", "parallelism": f"replicas x{world}",
+            "reference_sample": f"the reference arm and cpu_baseline time layer 1 ({n + n // 2} gates) of the "
+                                "circuit per step and report its GB/s; every layer has the same gate mix, so the "
+                                "rate stands for the whole circuit"}
 
 
 # ---------------------------------------------------------------------------
@@ -77,9 +81,35 @@ def cpu_sample(circ, n_gates):
     return Circuit(circ.gate_list()[:n_gates])
 
 
-def run_cpu_baseline(circ, n, n_gates):
+def compare_with_file(sv, path):
+    """(max |delta amp|, 1 - fidelity) of a device state against a raw
+    complex128 state file, streamed through the GPU 1 GiB at a time."""
+    import numpy as np
+    import oracle
+    import torch
+    x = sv.as_torch()
+    piece = 1 << 26
+    dmax, ov, nx, ny = 0.0, 0j, 0.0, 0.0
+    for i in range(0, x.numel(), piece):
+        r = torch.from_numpy(oracle.read_state_piece(path, i, min(piece, x.numel() - i))).to(x.device)
+        g = x[i:i + r.numel()].to(torch.complex128)
+        dmax = max(dmax, float((g - r).abs().max()))
+        ov += complex(torch.vdot(r, g))
+        nx += float(torch.vdot(g, g).real)
+        ny += float(torch.vdot(r, r).real)
+        del r, g
+    if not np.isfinite(dmax):
+        dmax = float("inf")
+    return dmax, max(0.0, 1.0 - abs(ov) ** 2 / (nx * ny))
+
+
+def run_cpu_baseline(circ, n, n_gates, check_gpu=False):
     """Time the reference (oracle/_ref) or, if it was not built, the oracle's C
-    port, on the first n_gates gates of the workload.  Returns a dict."""
+    port, on the first n_gates gates of the workload.  With check_gpu the
+    reference's final state of that sample (the full 2^n amplitudes) is also
+    compared with the GPU per-gate path's state for the same gates.  Returns a
+    dict."""
+    import tempfile
     import numpy as np
     import oracle
     from subquokka_dev_b200.circuits import algorithmic_bytes
@@ -93,9 +123,20 @@ def run_cpu_baseline(circ, n, n_gates):
         return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
                 "sample": f"skipped: host has less than {need >> 30} GiB available"}
     desc = f"first {n_gates} gates (layer 1) of the {n}-qubit circuit, runner span only"
+    parity = None
     if oracle.have_reference():
-        _, secs = oracle.run_reference(n, sample.to_text(), 0, init=None, chunk_qbit=12,
-                                       file_qbit=file_qbit)
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "ref_state.bin") if check_gpu else None
+            _, secs = oracle.run_reference(n, sample.to_text(), 0, init=None, chunk_qbit=12,
+                                           file_qbit=file_qbit, out_path=out)
+            if check_gpu:
+                from subquokka_dev_b200 import StateVector
+                with StateVector(n, "c128") as sv:
+                    sv.apply(sample)
+                    sv.synchronize()
+                    dmax, infid = compare_with_file(sv, out)
+                parity = {"gates": n_gates, "qubits": n, "max_abs_damp_gpu_vs_reference": dmax,
+                          "one_minus_fidelity": infid, "path": "per-gate complex128 (qk_apply_gates)"}
         kind = "reference"
     else:
         s = np.zeros(1 << n, np.complex128)
@@ -104,8 +145,11 @@ def run_cpu_baseline(circ, n, n_gates):
         oracle.apply_circuit(s, n, sample)
         secs = time.perf_counter() - t0
         kind, threads = "port", cores
-    return {"value": sbytes / secs / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": desc, "seconds": secs}
+    out = {"value": sbytes / secs / 1e9, "unit": UNIT, "cores": threads, "host_cores": cores, "kind": kind,
+           "sample": desc, "seconds": secs}
+    if parity is not None:
+        out["sample_parity"] = parity
+    return out
 
 
 def reference_arm(args, rank, world):
@@ -130,8 +174,8 @@ def reference_arm(args, rank, world):
             "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "impl": "reference", "config": config_dict(args, world),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
-                             "sample": cb["sample"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "host_cores": cb["host_cores"],
+                             "kind": cb["kind"], "sample": cb["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -359,19 +403,31 @@ def extra_workloads(args):
     circ, idx = pc.bind(params)
     res = {"qubits": n, "layers": layers, "params": pc.nparams, "gates": circ.ngates}
     grads = {}
+    peak, _ = measured_peak_hbm()
+    from subquokka_dev_b200 import last_sweep
     for dtype, fused in (("c128", False), ("c128", True), ("c64", True)):
         sv = StateVector(n, dtype)
         sv.set_stream(stream)
-        box = {}
+        box = {"dev": []}
 
         def run():
             sv.reset()
             box["r"] = adjoint_grad(sv, circ, idx, pc.nparams, terms, -1, fused)
+            box["dev"].append(last_sweep(sv))
         ms = time_device(run, 2, 3)
         ev, g, drift = box["r"]
         grads[(dtype, fused)] = g
         key = f"{dtype}_{'fused' if fused else 'per_gate'}"
-        res[key] = {"ms": ms, "grads_per_s": pc.nparams / (ms / 1e3), "expval": ev, "drift": drift}
+        # device span of the sweep itself (CUDA events inside the call, host
+        # planning excluded), median of the timed calls
+        dev = box["dev"][2:]
+        dms = statistics.median(d["device_ms"] for d in dev)
+        res[key] = {"ms": ms, "grads_per_s": pc.nparams / (ms / 1e3), "device_ms": dms,
+                    "grads_per_s_device": pc.nparams / (dms / 1e3), "expval": ev, "drift": drift,
+                    "forward_passes": dev[-1]["forward_passes"], "backward_passes": dev[-1]["backward_passes"]}
+        if dev[-1]["alg_bytes"] > 0:
+            gbs = dev[-1]["alg_bytes"] / (dms / 1e3) / 1e9
+            res[key].update({"alg_bytes": dev[-1]["alg_bytes"], "hbm_gbs": gbs, "hbm_frac": gbs / peak})
         sv.close()
     ref = grads[("c128", False)]
     for k, g in grads.items():
@@ -457,12 +513,15 @@ def extra_workloads(args):
     setup_s = time.perf_counter() - t0
     batch.run()
     torch.cuda.synchronize()
-    reps = 3
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
     t1 = time.perf_counter()
+    dev_ms = []
     for _ in range(reps):
         ev, grads, drift = batch.run()
+        dev_ms.append(batch.timing()[0])   # CUDA events around the graph launch
     wall_ms = (time.perf_counter() - t1) / reps * 1e3
+    bms = statistics.median(dev_ms)
+    balg = batch.timing()[1]
     # spot check against the single-circuit complex128 path
     from subquokka_dev_b200 import adjoint_grad as _adj
     errs = []
@@ -474,8 +533,12 @@ def extra_workloads(args):
         errs.append(float(np.abs(grads[c] - g).max() / np.abs(g).max()))
     st = batch.stats()
     nparams = sum(pc.nparams for pc, _, _ in items)
+    peak, _ = measured_peak_hbm()
     out["batch256_c64"] = {"circuits": 256, "params": nparams, "ms_per_batch": wall_ms,
                            "circuits_per_s": 256 / (wall_ms / 1e3), "grads_per_s": nparams / (wall_ms / 1e3),
+                           "device_ms_per_batch": bms, "circuits_per_s_device": 256 / (bms / 1e3),
+                           "grads_per_s_device": nparams / (bms / 1e3), "alg_bytes_per_batch": balg,
+                           "hbm_gbs": balg / (bms / 1e3) / 1e9, "hbm_frac": balg / (bms / 1e3) / 1e9 / peak,
                            "graph_steps": st["steps"], "launches_per_batch": st["launches"],
                            "tile_shape": [st["tile_bits"], st["reg_bits"], st["adj_tile_bits"], st["adj_reg_bits"]],
                            "setup_s_with_autotune": setup_s, "max_drift": float(drift.max()),
@@ -590,7 +653,7 @@ def our_arm(args, rank, world):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_baseline(circ, n, n + n // 2)
+        cpu = run_cpu_baseline(circ, n, n + n // 2, check_gpu=True)
         cpu.pop("seconds", None)
 
     if rank == 0:
@@ -601,10 +664,50 @@ def our_arm(args, rank, world):
                 "gates_per_s": world * circ.ngates / (ms_per_step / 1e3),
                 "hbm_frac_of_peak": value / peak,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-                "fused": variants, "workloads": extra,
-                "gpu_launches": launches}
+                "gpu_launches": launches, "fused": variants, "workloads": extra}
+        # last, so that a reader of the line's tail sees every target at once
+        line["summary"] = summarize(line, peak)
         print(json.dumps(line))
     return 0
+
+
+def summarize(line, peak):
+    """Compact view of the figures the targets are set on: the plain
+    complex128 path against HBM roofline, the fused forms' speed-up and error,
+    the adjoint and batch rates with their HBM fractions."""
+    r = lambda x, k=4: None if x is None else float(f"{x:.{k}g}")
+    out = {"plain_c128_s": r(line["circuit_seconds"]), "plain_c128_hbm_frac": r(line["hbm_frac_of_peak"], 3),
+           "plain_c128_kernel_frac": r(line["roofline"]["frac"], 3)}
+    f = line.get("fused") or {}
+    for key, name in (("c64_tensor_core", "fused_c64_tc"), ("c128", "fused_c128"), ("c64", "fused_c64")):
+        if key in f:
+            v = f[key]
+            out[name] = {"s": r(v["ms_per_circuit"] / 1e3), "x_vs_plain": r(v["speedup_vs_plain_c128"], 3),
+                         "one_minus_F": r(v["one_minus_fidelity_vs_c128"], 2),
+                         "max_damp": r(v["max_abs_damp_vs_c128"], 2), "hbm_frac": r(v["hbm_gbs_passes"] / peak, 3)}
+    w = line.get("workloads") or {}
+    h = w.get("hea26_adjoint")
+    if h:
+        out["hea26_adjoint"] = {k: {"grads_per_s": r(h[k]["grads_per_s"]), "device_ms": r(h[k]["device_ms"]),
+                                    "hbm_frac": r(h[k].get("hbm_frac"), 3),
+                                    "rel_err_vs_c128": r(h[k]["max_rel_grad_err_vs_c128_per_gate"], 2)}
+                                for k in ("c128_fused", "c64_fused") if k in h}
+    b = w.get("batch256_c64")
+    if b:
+        out["batch256_c64"] = {"circuits_per_s": r(b["circuits_per_s"]), "grads_per_s": r(b["grads_per_s"]),
+                               "device_ms": r(b["device_ms_per_batch"]), "hbm_frac": r(b["hbm_frac"], 3)}
+    q = w.get("random33_c64", {}).get("tensor_core_width6")
+    if q:
+        out["random33_c64_tc"] = {"s": r(q["ms_per_circuit"] / 1e3), "hbm_frac": r(q["hbm_gbs_passes"] / peak, 3),
+                                  "one_minus_F_28q": r(q["one_minus_fidelity_vs_c128"], 2)}
+    cb = line.get("cpu_baseline") or {}
+    if cb.get("value"):
+        out["cpu_reference_gbs"] = r(cb["value"])
+        out["cpu_threads"] = cb.get("cores")
+        sp = cb.get("sample_parity")
+        if sp:
+            out["parity_sample_max_damp_vs_reference"] = sp["max_abs_damp_gpu_vs_reference"]
+    return out
 
 
 def main():

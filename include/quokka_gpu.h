@@ -327,6 +327,16 @@ int qk_adjoint_grad_fused(qk_sv *sv, const qk_gate *gates, size_t ngates, const 
                           const qk_pauli_term *terms, size_t nterms, int checkpoints, double *expval, double *grad,
                           double *drift);
 
+/* No counterpart in the reference.  Device time of the last qk_adjoint_grad /
+ * qk_adjoint_grad_fused on sv (CUDA events on the state's stream, from its
+ * first device operation to its last; host planning excluded), the bytes its
+ * kernels and copies must read and write (fused sweeps: 2S per forward pass,
+ * 4S per two-state pass, plus the H application, reductions and checkpoint
+ * copies; 0 for the per-gate sweep, whose traffic is not counted), and its
+ * forward and backward pass (or, per-gate, launch) counts. */
+int qk_sv_last_sweep(const qk_sv *sv, double *device_ms, double *alg_bytes, int *forward_passes,
+                     int *backward_passes);
+
 /* ---- batches of variational circuits ------------------------------------ */
 /* No counterpart in the reference.  Many circuits of different sizes, each
  * with its own trainable RX/RY/RZ gates and Pauli-sum H: <H> and the adjoint
@@ -360,6 +370,11 @@ int qk_batch_set_params(qk_batch *b, const double *params);
 /* Graph steps, kernel launches per run and the chosen tile shapes. */
 int qk_batch_stats(const qk_batch *b, int *steps, int *launches, int *tile_bits, int *reg_bits, int *adj_tile_bits,
                    int *adj_reg_bits);
+/* Device time of the last qk_batch_run (CUDA events around the graph launch
+ * on the batch's stream) and the bytes one run must read and write: per
+ * circuit of S bytes, 2S per forward pass, 4S per two-state pass, S for the
+ * reset, 2S for lambda = H psi, S for the drift check. */
+int qk_batch_timing(const qk_batch *b, double *device_ms, double *alg_bytes);
 void qk_batch_destroy(qk_batch *b);
 
 /* ---- fused passes without device allocation --------------------------- */

@@ -87,8 +87,12 @@ def have_reference() -> bool:
 
 
 def run_reference(n: int, circuit_text: str, is_subcircuit: int, init: np.ndarray | None = None,
-                  chunk_qbit: int = 12, file_qbit: int = 0, threads: int | None = None):
-    """Run the unmodified reference MEM runner; returns (final state, runner seconds)."""
+                  chunk_qbit: int = 12, file_qbit: int = 0, threads: int | None = None,
+                  out_path: str | None = None):
+    """Run the unmodified reference MEM runner; returns (final state, runner
+    seconds).  With out_path the final state stays in that file (raw
+    complex128) and None is returned in its place: large states are then read
+    piece by piece (read_state_piece) instead of as one host array."""
     chunk = min(chunk_qbit, n - file_qbit)
     with tempfile.TemporaryDirectory() as d:
         ini = os.path.join(d, "x.ini")
@@ -98,7 +102,7 @@ def run_reference(n: int, circuit_text: str, is_subcircuit: int, init: np.ndarra
         cir = os.path.join(d, "c.txt")
         with open(cir, "w") as f:
             f.write(circuit_text)
-        out = os.path.join(d, "out.bin")
+        out = out_path or os.path.join(d, "out.bin")
         cmd = [REF_DRIVER, "-i", ini, "-c", cir, "-o", out]
         if init is not None:
             ip = os.path.join(d, "init.bin")
@@ -110,7 +114,14 @@ def run_reference(n: int, circuit_text: str, is_subcircuit: int, init: np.ndarra
         r = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
         m = re.search(r"^([0-9.eE+-]+)s$", r.stdout, re.M)
         secs = float(m.group(1)) if m else float("nan")
+        if out_path:
+            return None, secs
         return np.fromfile(out, dtype=np.complex128), secs
+
+
+def read_state_piece(path: str, first: int, count: int) -> np.ndarray:
+    """Amplitudes [first, first + count) of a raw complex128 state file."""
+    return np.fromfile(path, dtype=np.complex128, count=count, offset=16 * first)
 
 
 def pauli_expval(state: np.ndarray, n: int, terms) -> float:

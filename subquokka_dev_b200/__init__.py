@@ -7,10 +7,11 @@ is the Python side of that ABI: ctypes bindings (_lib), the runner mirror
 (engine) and the seeded workloads (circuits).
 """
 from .engine import (Batch, Circuit, Config, GateGraph, Plan, Simulator, StateVector, adjoint_grad, apply_gates_dev,
-                     chunk_groups, expval, gate_line, gate_matrix, make_gate, parse_line, pauli_terms, zz_x_hamiltonian)
+                     chunk_groups, expval, gate_line, gate_matrix, last_sweep, make_gate, parse_line, pauli_terms,
+                     zz_x_hamiltonian)
 from ._lib import QkError, load as load_library
 
 __all__ = ["Batch", "Circuit", "Config", "GateGraph", "Plan", "Simulator", "StateVector", "adjoint_grad", "apply_gates_dev",
-           "chunk_groups", "expval",
+           "chunk_groups", "expval", "last_sweep",
            "gate_line", "gate_matrix", "make_gate", "parse_line", "pauli_terms", "zz_x_hamiltonian", "QkError",
            "load_library"]

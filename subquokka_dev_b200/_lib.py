@@ -108,6 +108,8 @@ PROTOTYPES = {
     "qk_sv_set_stream": (c_int, [c_void_p, c_void_p]),
     "qk_sv_synchronize": (c_int, [c_void_p]),
     "qk_sv_release_workspace": (c_int, [c_void_p]),
+    "qk_sv_last_sweep": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double), POINTER(c_int), POINTER(c_int)]),
+    "qk_batch_timing": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
     "qk_apply_gates": (c_int, [c_void_p, POINTER(QkGate), c_size_t]),
     "qk_graph_create": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_void_p)]),
     "qk_graph_launch": (c_int, [c_void_p]),

@@ -263,6 +263,12 @@ static int adjoint_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, 
     double *dacc = ws.acc;
     int rc = QK_OK;
     const size_t nacc = nparams + 2;  // grads, expval, drift
+    e = ws.events();
+    if (e == cudaSuccess) e = cudaEventRecord(ws.ev0, st);
+    if (e != cudaSuccess) return cuda_err(e, "sweep timing events");
+    ws.last_fwd = ws.last_bwd = (int)ng;   // one launch per gate each way
+    ws.last_other = (int)(groups.size() + 1 + 3 * cpos.size());
+    ws.last_bytes = 0;                     // not counted for the per-gate sweep
     e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
     if (e != cudaSuccess) return cuda_err(e, "clear accumulators");
 
@@ -314,10 +320,16 @@ static int adjoint_t(C *psi, int n, int dtype, const qk_gate *gates, size_t ng, 
             if (e != cudaSuccess) return cuda_err(e, "restore checkpoint");
         }
     }
+    e = cudaEventRecord(ws.ev1, st);
+    if (e != cudaSuccess) return cuda_err(e, "sweep timing events");
     std::vector<double> h(nacc);
     e = cudaMemcpyAsync(h.data(), dacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_err(e, "read results");
+    {
+        float ms = 0;
+        ws.last_ms = cudaEventElapsedTime(&ms, ws.ev0, ws.ev1) == cudaSuccess ? ms : -1.0;
+    }
     if (grad) std::memcpy(grad, h.data(), nparams * sizeof(double));
     if (expval) *expval = h[nparams];
     if (drift) *drift = std::sqrt(h[nparams + 1]);
@@ -370,8 +382,25 @@ static int adjoint_fused_t(C *psi, int n, int dtype, const qk_gate *gates, size_
         if (!rc) rc = upload_host_plan(bwd[sgi], ws.plans[2 * sgi + 1], st);
         if (rc) return rc;
     }
+    e = ws.events();
+    if (e == cudaSuccess) e = cudaEventRecord(ws.ev0, st);
+    if (e != cudaSuccess) return cuda_err(e, "sweep timing events");
     e = cudaMemsetAsync(dacc, 0, nacc * sizeof(double), st);
     if (e != cudaSuccess) return cuda_err(e, "clear accumulators");
+    // algorithmic traffic: a forward pass reads and writes psi (2S), a
+    // two-state pass psi and lambda (4S); lambda = H psi reads psi and writes
+    // lambda (2S) and every further Pauli group re-reads lambda (3S); <H>
+    // reads both (2S); each checkpoint copy, drift check and restore 2S
+    ws.last_fwd = ws.last_bwd = ws.last_other = 0;
+    for (size_t sgi = 0; sgi < nseg; ++sgi) {
+        ws.last_fwd += (int)fwd[sgi].passes.size();
+        ws.last_bwd += (int)bwd[sgi].passes.size();
+    }
+    const double S = (double)bytes;
+    const double ng_h = groups.empty() ? 1.0 : (double)groups.size();
+    ws.last_other = (int)(ng_h + 1 + 3 * (nseg - 1));
+    ws.last_bytes = 2 * S * ws.last_fwd + 4 * S * ws.last_bwd + (groups.empty() ? S : 2 * S + 3 * S * (ng_h - 1)) +
+                    2 * S + 3 * 2 * S * (double)(nseg - 1);
     // forward
     for (size_t sgi = 0; sgi < nseg; ++sgi) {
         if (sgi > 0) {
@@ -394,10 +423,16 @@ static int adjoint_fused_t(C *psi, int n, int dtype, const qk_gate *gates, size_
             if (e != cudaSuccess) return cuda_err(e, "restore checkpoint");
         }
     }
+    e = cudaEventRecord(ws.ev1, st);
+    if (e != cudaSuccess) return cuda_err(e, "sweep timing events");
     std::vector<double> h(nacc);
     e = cudaMemcpyAsync(h.data(), dacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_err(e, "read results");
+    {
+        float ms = 0;
+        ws.last_ms = cudaEventElapsedTime(&ms, ws.ev0, ws.ev1) == cudaSuccess ? ms : -1.0;
+    }
     if (grad) std::memcpy(grad, h.data(), nparams * sizeof(double));
     if (expval) *expval = h[nparams];
     if (drift) *drift = std::sqrt(h[nparams + 1]);

@@ -243,6 +243,9 @@ struct qk_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     size_t launches = 0;
+    // qk_batch_timing: events around the last graph launch, algorithmic bytes of one run
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0, alg_bytes = 0;
 
     // programs, step tables, coefficient buffer and graph (rebuilt per tile shape)
     void free_plans() {
@@ -279,6 +282,8 @@ struct qk_batch {
     }
     ~qk_batch() {
         free_device();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -311,6 +316,14 @@ static int build_tables(qk_batch *b) {
     const TOp *fops = b->fdev.ops, *bops = b->bdev.ops;
     const C *fcoef = (const C *)b->fdev.coef, *bcoef = (const C *)b->bdev.coef;
     double *grads = b->d_out;
+    // algorithmic traffic of one run: per circuit of S bytes, a forward pass
+    // 2S, a two-state pass 4S, the reset S, lambda = H psi 2S (psi read,
+    // lambda written), the drift check S
+    b->alg_bytes = 0;
+    for (int c = 0; c < b->ncirc; ++c) {
+        const double S = (double)sizeof(C) * (double)(1ull << b->n[c]);
+        b->alg_bytes += S * (2.0 * b->fplan[c].passes.size() + 4.0 * b->bplan[c].passes.size() + 4.0);
+    }
     for (int ns = 1; ns <= 2; ++ns) {
         const size_t kmax = ns == 1 ? fmax : bmax;
         for (size_t k = 0; k < kmax; ++k) {
@@ -727,9 +740,16 @@ int qk_batch_create(int ncirc, const int32_t *nqubits, const qk_gate *gates, con
 
 int qk_batch_run(qk_batch *b, double *expvals, double *grads, double *drift) {
     if (!b) return fail(QK_ERR_ARG, "null batch");
-    cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+    cudaError_t e = cudaSuccess;
+    if (!b->ev0) e = cudaEventCreate(&b->ev0);
+    if (e == cudaSuccess && !b->ev1) e = cudaEventCreate(&b->ev1);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev0, b->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, b->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return cuda_err(e, "batch run");
+    float ms = 0;
+    b->last_ms = cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess ? ms : -1.0;
     if (grads) std::memcpy(grads, b->h_out, b->nparams * sizeof(double));
     if (expvals) std::memcpy(expvals, b->h_out + b->nparams, b->ncirc * sizeof(double));
     if (drift)
@@ -757,6 +777,13 @@ int qk_batch_set_params(qk_batch *b, const double *params) {
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return cuda_err(e, "batch sync");
     fill_coefficients(b);
+    return QK_OK;
+}
+
+int qk_batch_timing(const qk_batch *b, double *device_ms, double *alg_bytes) {
+    if (!b) return fail(QK_ERR_ARG, "null batch");
+    if (device_ms) *device_ms = b->last_ms;
+    if (alg_bytes) *alg_bytes = b->alg_bytes;
     return QK_OK;
 }
 

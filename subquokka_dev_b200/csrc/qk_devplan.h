@@ -36,6 +36,18 @@ struct Workspace {
     double *acc = nullptr;       // gradient / <H> / drift accumulators
     size_t acc_cap = 0;          // bytes
     std::vector<DevPlan> plans;  // device programs of the sweep's passes
+    // device time and traffic of the last sweep (qk_sv_last_sweep)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0, last_bytes = 0;
+    int last_fwd = 0, last_bwd = 0, last_other = 0;
+
+    // Timing events, created on first use.
+    cudaError_t events() {
+        cudaError_t e = cudaSuccess;
+        if (!ev0) e = cudaEventCreate(&ev0);
+        if (e == cudaSuccess && !ev1) e = cudaEventCreate(&ev1);
+        return e;
+    }
 
     // Make room for `states_bytes` of states, `acc_bytes` of accumulators and
     // `nplans` device plans.  Returns a cudaError_t.
@@ -67,6 +79,9 @@ struct Workspace {
         states_cap = acc_cap = 0;
         for (auto &p : plans) p.release();
         plans.clear();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        ev0 = ev1 = nullptr;
     }
 };
 

@@ -201,6 +201,18 @@ int qk_sv_release_workspace(qk_sv *sv) {
     return QK_OK;
 }
 
+int qk_sv_last_sweep(const qk_sv *sv, double *device_ms, double *alg_bytes, int *forward_passes,
+                     int *backward_passes) {
+    if (!sv) return fail(QK_ERR_ARG, "null state");
+    if (!sv->ws.ev0) return fail(QK_ERR_ARG, "no adjoint sweep has run on this state");
+    if (device_ms) *device_ms = sv->ws.last_ms;
+    if (alg_bytes) *alg_bytes = sv->ws.last_bytes;
+    if (forward_passes) *forward_passes = sv->ws.last_fwd;
+    if (backward_passes) *backward_passes = sv->ws.last_bwd;
+    clear_error();
+    return QK_OK;
+}
+
 int qk_sv_reset(qk_sv *sv) {
     if (!sv) return fail(QK_ERR_ARG, "null state");
     const uint64_t namp = 1ull << sv->n;

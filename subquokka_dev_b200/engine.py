@@ -392,6 +392,14 @@ def adjoint_grad(sv: "StateVector", circuit: Circuit, param_index, nparams: int,
     return ev.value, grad[:nparams], drift.value
 
 
+def last_sweep(sv: "StateVector") -> dict:
+    """Device time (ms, CUDA events), algorithmic bytes (0 = not counted) and
+    pass counts of the last adjoint sweep on sv (qk_sv_last_sweep)."""
+    ms, nb, f, b = c_double(), c_double(), c_int(), c_int()
+    check(_lib.load().qk_sv_last_sweep(sv.h, byref(ms), byref(nb), byref(f), byref(b)))
+    return {"device_ms": ms.value, "alg_bytes": nb.value, "forward_passes": f.value, "backward_passes": b.value}
+
+
 class Batch:
     """Many variational circuits, <H> and adjoint gradients of each, from one
     CUDA graph (qk_batch_*).  items: [(ParamCircuit, params, terms), ...]."""
@@ -441,6 +449,12 @@ class Batch:
     def set_params(self, params_per_circuit) -> None:
         flat = np.concatenate([np.asarray(p, dtype=np.float64) for p in params_per_circuit])
         check(self._lib.qk_batch_set_params(self.h, flat.ctypes.data_as(POINTER(c_double))))
+
+    def timing(self):
+        """(device ms of the last run, algorithmic bytes of one run) (qk_batch_timing)."""
+        ms, nb = c_double(), c_double()
+        check(self._lib.qk_batch_timing(self.h, byref(ms), byref(nb)))
+        return ms.value, nb.value
 
     def stats(self):
         v = [c_int() for _ in range(6)]
