@@ -40,6 +40,9 @@ def build(with_reference: bool | None = None, ref_dir: str | None = None) -> Non
         with_reference = have_reference_source(d)
     if with_reference:
         subprocess.run(["make", "-C", ORACLE_DIR, "ref", "-j8", f"REF={d}"], check=True)
+        # the reference CLI with the engine in its GPU slot (needs the built library)
+        if os.path.exists(os.path.join(ORACLE_DIR, "..", "subquokka_dev_b200", "lib", "libquokka_gpu.so")):
+            subprocess.run(["make", "-C", ORACLE_DIR, "ref-gpu", f"REF={d}"], check=True)
 
 
 def load():
