@@ -547,6 +547,33 @@ def extra_workloads(args):
     return out
 
 
+def sharded_batch(world):
+    """The 256-circuit batch (complex64, forward + adjoint) split over all
+    ranks by cost (subquokka_dev_b200.sharding): each rank runs one CUDA graph
+    over its circuits, one all-reduce gathers every result on every rank.
+    circuits/s = 256 / the slowest rank's device time (strong scaling: the
+    batch is fixed, the ranks share it)."""
+    import torch
+    from subquokka_dev_b200 import circuits
+    from subquokka_dev_b200.sharding import ShardedBatch
+    items = circuits.variational_batch(256, 2025)
+    sb = ShardedBatch(items, "c64", device=torch.device("cuda", torch.cuda.current_device()))
+    for _ in range(2):
+        sb.run()
+    ms = []
+    for _ in range(5):
+        sb.run()
+        ms.append(sb.device_ms())
+    local = statistics.median(ms)
+    worst = max_over_ranks(local, world)
+    nparams = sum(pc.nparams for pc, _, _ in items)
+    out = {"circuits": 256, "ranks": world, "scaling": "strong", "circuits_on_rank0": len(sb.mine),
+           "max_rank_device_ms": worst, "circuits_per_s": 256 / (worst / 1e3), "grads_per_s": nparams / (worst / 1e3),
+           "collective": "one all_reduce of the results per run (no data-path exchange)"}
+    sb.close()
+    return out
+
+
 def our_arm(args, rank, world):
     import numpy as np
     import torch
@@ -620,6 +647,9 @@ def our_arm(args, rank, world):
     launches = args.steps * (circ.ngates + 1)
     variants = {} if args.no_fused else fused_variants(args, circ, sv, ms_per_step, alg)
     extra = {} if (args.no_extra or rank != 0) else None
+    sharded = None
+    if world > 1 and not args.no_extra:
+        sharded = sharded_batch(world)   # every rank takes part
 
     # end to end through the public API: host gate records in, final state out to pinned host memory
     e2e = None
@@ -665,6 +695,8 @@ def our_arm(args, rank, world):
                 "hbm_frac_of_peak": value / peak,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches, "fused": variants, "workloads": extra}
+        if sharded is not None:
+            line["batch256_sharded"] = sharded
         # last, so that a reader of the line's tail sees every target at once
         line["summary"] = summarize(line, peak)
         print(json.dumps(line))
