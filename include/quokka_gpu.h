@@ -401,6 +401,40 @@ void qk_batch_destroy(qk_batch *b);
  * returning, and a call on a stream under capture returns QK_ERR_UNSUPPORTED. */
 int qk_apply_fused_noalloc(void *state, int nqubits, int dtype, const qk_gate *gates, size_t n, void *cuda_stream);
 
+/* ---- states larger than HBM: host memory, GPU compute ------------------- */
+
+typedef struct qk_hsv qk_hsv;   /* host-resident state vector */
+
+/* Replaces IO_Runner (src/IO_Runner.cpp:309-488, state in files, chunks of
+ * 2^chunk_qbit run on the host cores) for states that do not fit in HBM: the
+ * 2^nqubits amplitudes of dtype live in pinned host memory (index k = the
+ * in-memory layout, never permuted), and the GPU holds three buffers of
+ * 2^chunk_qubits amplitudes.  Starts in |0...0>. */
+int qk_hsv_create(int nqubits, int chunk_qubits, int dtype, qk_hsv **out);
+/* |0...0> again. */
+int qk_hsv_reset(qk_hsv *h);
+/* The host amplitudes: 2^nqubits interleaved (re, im) doubles (complex128)
+ * or floats (complex64); read or write them between calls. */
+void *qk_hsv_data(qk_hsv *h);
+/* Apply gates[0..n).  The gates are cut into segments whose qubits fit in
+ * chunk_qubits "local" qubits; each segment is one sweep that copies every
+ * chunk (the amplitudes sharing one value of the other qubits) to the GPU,
+ * runs the segment's fused passes on it and copies it back, copies and
+ * compute overlapped on three streams.  A qubit enters the local set by a
+ * change of the copy addresses, not by moving amplitudes (the reference's
+ * VSWAP).  Synchronous: returns when the host state holds the result. */
+int qk_hsv_apply_gates(qk_hsv *h, const qk_gate *gates, size_t n);
+/* Segments of the last qk_hsv_apply_gates, its device time (CUDA events from
+ * the first copy-in to the last copy-out) and the bytes it moved over the
+ * host link (2 x state bytes per segment). */
+int qk_hsv_stats(const qk_hsv *h, int *segments, double *device_ms, double *link_bytes);
+void qk_hsv_destroy(qk_hsv *h);
+/* The segmentation qk_hsv_apply_gates uses (host only): *nsegments; when it
+ * is <= cap, per segment its local qubit mask and gate count, and in order[]
+ * (n entries) the gate indices in execution order, segment after segment. */
+int qk_ooc_segments(const qk_gate *gates, size_t n, int nqubits, int chunk_qubits, uint64_t *local_masks,
+                    int32_t *segment_sizes, int32_t *order, size_t cap, size_t *nsegments);
+
 /* Run a parsed circuit the way Simulator::run does (src/simulator.cpp:671-706):
  * groups if cfg->is_subcircuit, else gates (fused passes if cfg->fuse_width >
  * 0); *seconds receives the device time of the runner span alone. */

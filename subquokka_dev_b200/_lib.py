@@ -110,6 +110,14 @@ PROTOTYPES = {
     "qk_sv_release_workspace": (c_int, [c_void_p]),
     "qk_sv_last_sweep": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double), POINTER(c_int), POINTER(c_int)]),
     "qk_batch_timing": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+    "qk_hsv_create": (c_int, [c_int, c_int, c_int, POINTER(c_void_p)]),
+    "qk_hsv_reset": (c_int, [c_void_p]),
+    "qk_hsv_data": (c_void_p, [c_void_p]),
+    "qk_hsv_apply_gates": (c_int, [c_void_p, POINTER(QkGate), c_size_t]),
+    "qk_hsv_stats": (c_int, [c_void_p, POINTER(c_int), POINTER(c_double), POINTER(c_double)]),
+    "qk_hsv_destroy": (None, [c_void_p]),
+    "qk_ooc_segments": (c_int, [POINTER(QkGate), c_size_t, c_int, c_int, POINTER(ctypes.c_uint64), POINTER(c_int32),
+                                POINTER(c_int32), c_size_t, POINTER(c_size_t)]),
     "qk_apply_gates": (c_int, [c_void_p, POINTER(QkGate), c_size_t]),
     "qk_graph_create": (c_int, [c_void_p, POINTER(QkGate), c_size_t, POINTER(c_void_p)]),
     "qk_graph_launch": (c_int, [c_void_p]),

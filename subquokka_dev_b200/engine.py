@@ -392,6 +392,74 @@ def adjoint_grad(sv: "StateVector", circuit: Circuit, param_index, nparams: int,
     return ev.value, grad[:nparams], drift.value
 
 
+class HostStateVector:
+    """A state too large for HBM (qk_hsv_*): 2^n amplitudes in pinned host
+    memory, the gates run on the GPU chunk by chunk, 2^chunk_qubits
+    amplitudes at a time.  The replacement of the reference's IO runner
+    (src/IO_Runner.cpp:309-488)."""
+
+    def __init__(self, nqubits: int, chunk_qubits: int, dtype="c128"):
+        self._lib = _lib.load()
+        self.h = c_void_p()
+        check(self._lib.qk_hsv_create(int(nqubits), int(chunk_qubits), DTYPES[dtype], byref(self.h)))
+        self.nqubits, self.chunk_qubits, self.dtype = int(nqubits), int(chunk_qubits), DTYPES[dtype]
+
+    def view(self) -> np.ndarray:
+        """Zero-copy numpy view of the host amplitudes (complex128 / complex64)."""
+        ct = ctypes.c_double if self.dtype == QK_C128 else ctypes.c_float
+        p = ctypes.cast(self._lib.qk_hsv_data(self.h), POINTER(ct))
+        a = np.ctypeslib.as_array(p, shape=(2 << self.nqubits,))
+        return a.view(np.complex128 if self.dtype == QK_C128 else np.complex64)
+
+    def reset(self) -> None:
+        check(self._lib.qk_hsv_reset(self.h))
+
+    def apply(self, circuit: Circuit) -> None:
+        check(self._lib.qk_hsv_apply_gates(self.h, circuit.gates, circuit.ngates))
+
+    def stats(self) -> dict:
+        sg, ms, nb = c_int(), c_double(), c_double()
+        check(self._lib.qk_hsv_stats(self.h, byref(sg), byref(ms), byref(nb)))
+        return {"segments": sg.value, "device_ms": ms.value, "link_bytes": nb.value}
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.qk_hsv_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def ooc_segments(circuit: Circuit, nqubits: int, chunk_qubits: int):
+    """The segments qk_hsv_apply_gates would run: [(local qubit mask, [gate
+    indices in execution order]), ...] (host only)."""
+    lib = _lib.load()
+    ns = c_size_t()
+    check(lib.qk_ooc_segments(circuit.gates, circuit.ngates, int(nqubits), int(chunk_qubits), None, None, None, 0,
+                              byref(ns)))
+    k = ns.value
+    masks = (ctypes.c_uint64 * max(1, k))()
+    sizes = (c_int32 * max(1, k))()
+    order = (c_int32 * max(1, circuit.ngates))()
+    check(lib.qk_ooc_segments(circuit.gates, circuit.ngates, int(nqubits), int(chunk_qubits), masks, sizes, order,
+                              k, byref(ns)))
+    out, pos = [], 0
+    for i in range(k):
+        out.append((int(masks[i]), [int(order[pos + j]) for j in range(sizes[i])]))
+        pos += sizes[i]
+    return out
+
+
 def last_sweep(sv: "StateVector") -> dict:
     """Device time (ms, CUDA events), algorithmic bytes (0 = not counted) and
     pass counts of the last adjoint sweep on sv (qk_sv_last_sweep)."""
