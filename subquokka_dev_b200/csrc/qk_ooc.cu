@@ -136,6 +136,7 @@ struct qk_hsv {
     cudaEvent_t t0 = nullptr, t1 = nullptr, seg_done = nullptr;
     double last_ms = 0, last_bytes = 0;
     int last_segments = 0;
+    size_t max_pitch = 0;            // cudaDevAttrMaxPitch
     std::vector<DevPlan> plans;
 
     ~qk_hsv() {
@@ -190,19 +191,24 @@ int copy_chunk(qk_hsv *h, void *dev, uint64_t local, uint64_t base, bool to_devi
     if (nrest > 65536) return fail(QK_ERR_UNSUPPORTED, "chunk gather of %zu copies: too fragmented", nrest);
     unsigned char *hb = static_cast<unsigned char *>(h->host);
     unsigned char *db = static_cast<unsigned char *>(dev);
+    // a 2D copy takes pitches up to the device's limit; past it (rows of
+    // GiB), one plain copy per row
+    const bool two_d = rows > 1 && spitch <= h->max_pitch && width <= h->max_pitch;
+    const size_t per = two_d ? 1 : rows;
     for (size_t j = 0; j < nrest; ++j) {
         const uint64_t hoff = base | deposit(j, rest);
         const size_t doff = (j * rows) << r;     // device index of the first row
-        cudaError_t e;
-        if (to_device)
-            e = rows == 1 ? cudaMemcpyAsync(db + doff * es, hb + hoff * es, width, cudaMemcpyHostToDevice, st)
-                          : cudaMemcpy2DAsync(db + doff * es, width, hb + hoff * es, spitch, width, rows,
-                                              cudaMemcpyHostToDevice, st);
-        else
-            e = rows == 1 ? cudaMemcpyAsync(hb + hoff * es, db + doff * es, width, cudaMemcpyDeviceToHost, st)
-                          : cudaMemcpy2DAsync(hb + hoff * es, spitch, db + doff * es, width, width, rows,
-                                              cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) return cuda_e(e, to_device ? "chunk gather" : "chunk scatter");
+        for (size_t t = 0; t < per; ++t) {
+            unsigned char *hp = hb + (hoff + ((uint64_t)t << r0)) * es, *dp = db + (doff + (t << r)) * es;
+            cudaError_t e;
+            if (to_device)
+                e = two_d ? cudaMemcpy2DAsync(dp, width, hp, spitch, width, rows, cudaMemcpyHostToDevice, st)
+                          : cudaMemcpyAsync(dp, hp, width, cudaMemcpyHostToDevice, st);
+            else
+                e = two_d ? cudaMemcpy2DAsync(hp, spitch, dp, width, width, rows, cudaMemcpyDeviceToHost, st)
+                          : cudaMemcpyAsync(hp, dp, width, cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return cuda_e(e, to_device ? "chunk gather" : "chunk scatter");
+        }
     }
     return QK_OK;
 }
@@ -235,6 +241,10 @@ int qk_hsv_create(int nqubits, int chunk_qubits, int dtype, qk_hsv **out) {
     if (e == cudaSuccess) e = cudaEventCreate(&h->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&h->t1);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->seg_done, cudaEventDisableTiming);
+    int dev = 0, mp = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&mp, cudaDevAttrMaxPitch, dev);
+    h->max_pitch = mp > 0 ? (size_t)mp : 0;
     if (e != cudaSuccess) {
         const int rc = cuda_e(e, "host state / chunk buffers");
         delete h;
