@@ -504,6 +504,11 @@ def extra_workloads(args):
     sv.close()
     out["tensor_core_blocks_28q"] = lay
 
+    # host-resident state: the 32-qubit random circuit (20 layers) with the
+    # state in pinned host memory (64 GiB c128) and 2^29-amplitude chunks on
+    # the GPU (3 x 8 GiB); checked against the same circuit's fused plan in HBM
+    out["host_state_32q_c128"] = host_state_workload(32, 29)
+
     # batch of 256 variational circuits (14-22 qubits, 4-16 layers), complex64,
     # forward + <H> + adjoint gradients from one CUDA graph; tile shapes autotuned
     from subquokka_dev_b200 import Batch
@@ -572,6 +577,50 @@ def sharded_batch(world):
            "collective": "one all_reduce of the results per run (no data-path exchange)"}
     sb.close()
     return out
+
+
+def host_state_workload(n, L):
+    """qk_hsv_*: a state in pinned host memory, the gates on the GPU chunk by
+    chunk; device time (CUDA events, first copy-in to last copy-out), the
+    bytes moved over the host link, and the in-HBM fused plan of the same
+    circuit for comparison (max |delta amp| between the two)."""
+    import numpy as np
+    import torch
+    from subquokka_dev_b200 import HostStateVector, Plan, StateVector, circuits
+    need = (16 << n) + (24 << 30)
+    if mem_available_bytes() < need:
+        return {"skipped": f"host has less than {need >> 30} GiB available"}
+    circ = circuits.random_u3_cz(n, 20, SEED)
+    t0 = time.perf_counter()
+    hs = HostStateVector(n, L, "c128")
+    setup_s = time.perf_counter() - t0
+    hs.apply(circ)
+    st = hs.stats()
+    res = {"qubits": n, "chunk_qubits": L, "gates": circ.ngates, "state_bytes": 16 << n, "segments": st["segments"],
+           "device_ms": st["device_ms"], "link_bytes": st["link_bytes"],
+           "link_gbs_both_directions": st["link_bytes"] / (st["device_ms"] / 1e3) / 1e9,
+           "setup_s_pinned_alloc": setup_s}
+    sv = StateVector(n, "c128")
+    sv.set_stream(torch.cuda.current_stream().cuda_stream)
+    plan = Plan(circ, n, "c128")
+
+    def run():
+        sv.reset()
+        plan.apply(sv)
+    res["in_hbm_fused_ms"] = time_device(run, 1, 1)
+    host = hs.view()
+    x = sv.as_torch()
+    piece = 1 << 26
+    dmax = 0.0
+    for i in range(0, x.numel(), piece):
+        h = torch.from_numpy(host[i:i + piece]).to(x.device)
+        dmax = max(dmax, float((h - x[i:i + piece]).abs().max()))
+        del h
+    res["max_abs_damp_vs_in_hbm"] = dmax
+    plan.close()
+    sv.close()
+    hs.close()
+    return res
 
 
 def our_arm(args, rank, world):
@@ -732,6 +781,12 @@ def summarize(line, peak):
     if q:
         out["random33_c64_tc"] = {"s": r(q["ms_per_circuit"] / 1e3), "hbm_frac": r(q["hbm_gbs_passes"] / peak, 3),
                                   "one_minus_F_28q": r(q["one_minus_fidelity_vs_c128"], 2)}
+    hs = w.get("host_state_32q_c128")
+    if hs and "segments" in hs:
+        out["host_state_32q_c128"] = {"s": r(hs["device_ms"] / 1e3), "segments": hs["segments"],
+                                      "link_gbs": r(hs["link_gbs_both_directions"]),
+                                      "in_hbm_s": r(hs["in_hbm_fused_ms"] / 1e3),
+                                      "max_damp_vs_in_hbm": r(hs["max_abs_damp_vs_in_hbm"], 2)}
     cb = line.get("cpu_baseline") or {}
     if cb.get("value"):
         out["cpu_reference_gbs"] = r(cb["value"])

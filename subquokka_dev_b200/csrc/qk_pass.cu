@@ -29,8 +29,8 @@ namespace qk {
 // NS = 2 runs an adjoint pass over psi (s) and lambda (s2) together; the
 // gradient accumulators of the pass live in shared memory and are added to
 // ggrad[gparams[grad0 + i]] once per CTA.
-template <typename C, int R, int NS>
-__global__ void __launch_bounds__(pass_max_threads<C, R, NS>()) k_pass(C *__restrict__ s, C *__restrict__ s2, uint64_t ntiles,
+template <typename C, int R, int NS, bool NARROW>
+__global__ void __launch_bounds__(NARROW ? 128 : pass_max_threads<C, R, NS>(), NARROW ? 3 : 1) k_pass(C *__restrict__ s, C *__restrict__ s2, uint64_t ntiles,
                                                        const __grid_constant__ PassDesc d, const TOp *__restrict__ gprog,
                                                        const C *__restrict__ gcoef, const int32_t *__restrict__ gparams,
                                                        double *__restrict__ ggrad, int nbuf) {
@@ -149,28 +149,35 @@ template <typename C> struct PassArgs {
     double *ggrad;           // gradient accumulators (two-state passes)
 };
 
-template <typename C, int R, int NS>
-static int launch_pass_r(const PassArgs<C> &a, int n, const PassDesc &d, cudaStream_t st) {
+template <typename C, int R, int NS, bool NARROW>
+static int launch_pass_k(const PassArgs<C> &a, int n, const PassDesc &d, uint32_t threads, cudaStream_t st) {
     static std::atomic<uint64_t> smem_done{0};
     const size_t tile = (sizeof(C) << d.T) * NS;
     const int nbuf = d.perm ? 1 : (2 * tile <= (200u << 10) ? 2 : 1);
     const size_t smem = tile * nbuf + d.nprog * sizeof(TOp) + d.ncoef * sizeof(C) + (NS == 2 ? d.ngrad * sizeof(double) : 0);
     if (smem > (220u << 10)) return fail(QK_ERR_ARG, "pass needs %zu bytes of shared memory", smem);
     cudaError_t e;
-    e = smem_limit_once(smem_done, (const void *)k_pass<C, R, NS>, 220 << 10);
+    e = smem_limit_once(smem_done, (const void *)k_pass<C, R, NS, NARROW>, 220 << 10);
     if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(k_pass)");
     const int sms = device_sms();
-    const uint32_t threads = d.perm ? std::max<uint32_t>(1, std::min<uint32_t>(kPassThreads, 1u << d.T))
-                                    : (uint32_t)((1u << d.T) / R);
-    if (threads > kPassThreads || threads == 0) return fail(QK_ERR_ARG, "pass of %d tile bits needs %u threads", d.T, threads);
     int mb = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass<C, R, NS>, (int)threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass<C, R, NS, NARROW>, (int)threads, smem);
     if (e != cudaSuccess || mb < 1) mb = 1;
     const uint64_t ntiles = 1ull << (n - d.T);
     const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sms * mb);
-    k_pass<C, R, NS><<<grid, threads, smem, st>>>(a.s, a.s2, ntiles, d, a.ops, a.coef, a.gparams, a.ggrad, nbuf);
+    k_pass<C, R, NS, NARROW><<<grid, threads, smem, st>>>(a.s, a.s2, ntiles, d, a.ops, a.coef, a.gparams, a.ggrad, nbuf);
     e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_err(e, "k_pass launch");
+}
+
+template <typename C, int R, int NS>
+static int launch_pass_r(const PassArgs<C> &a, int n, const PassDesc &d, cudaStream_t st) {
+    const uint32_t threads = d.perm ? std::max<uint32_t>(1, std::min<uint32_t>(kPassThreads, 1u << d.T))
+                                    : (uint32_t)((1u << d.T) / R);
+    if (threads > kPassThreads || threads == 0) return fail(QK_ERR_ARG, "pass of %d tile bits needs %u threads", d.T, threads);
+    if constexpr (pass_narrow_ok<C, R, NS>())
+        if (!d.perm && threads <= 128) return launch_pass_k<C, R, NS, true>(a, n, d, threads, st);
+    return launch_pass_k<C, R, NS, false>(a, n, d, threads, st);
 }
 
 template <typename C>
