@@ -25,8 +25,6 @@ enum OpKind : int32_t {
     OP_GRAD = 8,    // adjoint sweep: grad[aux] += Im <lambda|G|psi>, G on q[0] = X/Y/Z by m[0] = 1/2/3
     OP_CX = 9,      // flip bit q[1 - aux] where bit q[aux] is set (a U2 that is exactly a CNOT)
     OP_CDENSE1 = 10,  // 2x2 on q[0]: m[0..7] where bit q[1] is 0, m[8..15] where it is 1 (planner-made)
-    OP_REAL1 = 11,  // real 2x2 on q[0], m[0..3] row-major reals              (planner-made)
-    OP_REAL2 = 12,  // real 4x4 on (q[0], q[1]), index bit0 = q[0], m[0..15]   (planner-made)
 };
 
 struct Op {
@@ -87,10 +85,6 @@ enum TOpKind : uint8_t {
     TOP_GRAD = 5,   // two-state passes: gacc[coef] += Im <lambda|G|psi>, G = X/Y/Z (b = 1/2/3) on slot a
     TOP_CX = 6,     // swap register slot a's pairs where qubit code b is 1 (controlled X)
     TOP_CG1 = 7,    // dense 2x2 on slot a: coef[0..3] or coef[4..7] by qubit code b (not a register slot)
-    TOP_R1 = 8,     // real 2x2 on slot a: coef[0..1] hold the 4 reals (a, b), (c, d), row-major
-    TOP_R2 = 9,     // real 4x4 on slots a < b (index bit0 = a): coef[0..7] hold the 16 reals, row-major
-    TOP_PHASES = 10,  // diagonal: amplitude *= product of the a TOP_TERM records that follow
-    TOP_TERM = 11,  // one factor of a TOP_PHASES: coef[bit(a) + 2 bit(b)] (codes a, b, slots bits[0], bits[1])
 };
 
 // Qubit codes of TOP_DIAG / TOP_PHASE: < 0x80 tile-local bit; 0x80 | q global
@@ -151,7 +145,6 @@ void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]);
 void asap_order(std::vector<Op> &ops, int n);
 void merge_one_qubit_runs(std::vector<Op> &ops, int n);
 void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n);
-void split_real(std::vector<Op> &ops);
 void hoist_gradients(std::vector<Op> &ops, int n);
 void pair_gradients(std::vector<Op> &ops);
 void relabel_perms(std::vector<Op> &ops, int n, int L, int max_bits, int max_pairs, bool swaps);

@@ -116,59 +116,6 @@ __device__ __forceinline__ void reg_g2(C (&v)[R], const C *__restrict__ m) {
 }
 
 
-// Real 2x2 on register slot S (a planner-split dense op: the complex phases
-// went to diagonal ops): c01 = (a, b), c23 = (c, d), [a b; c d] row-major.
-// Two real multiply-adds per output component instead of four.
-template <int S, typename C, int R>
-__device__ __forceinline__ void reg_r1(C (&v)[R], const C c01, const C c23) {
-    if constexpr ((1 << S) < R) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (k & (1 << S)) continue;
-            const C a = v[k], b = v[k | (1 << S)];
-            C x, y;
-            x.x = fma(c01.x, a.x, c01.y * b.x);
-            x.y = fma(c01.x, a.y, c01.y * b.y);
-            y.x = fma(c23.x, a.x, c23.y * b.x);
-            y.y = fma(c23.x, a.y, c23.y * b.y);
-            v[k] = x;
-            v[k | (1 << S)] = y;
-        }
-    }
-}
-
-// Real 4x4 on register slots A < B (index bit 0 = slot A): the 16 reals,
-// row-major, packed two to a complex coefficient m[0..7].
-template <int A, int B, typename C, int R>
-__device__ __forceinline__ void reg_r2(C (&v)[R], const C *__restrict__ m) {
-    if constexpr (A < B && (1 << B) < R) {
-        using T = decltype(v[0].x);
-        T M[16];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const C c = m[i];
-            M[2 * i] = c.x;
-            M[2 * i + 1] = c.y;
-        }
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (k & ((1 << A) | (1 << B))) continue;
-            const int k1 = k | (1 << A), k2 = k | (1 << B), k3 = k | (1 << A) | (1 << B);
-            const C x0 = v[k], x1 = v[k1], x2 = v[k2], x3 = v[k3];
-            C y[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                y[r].x = fma(M[4 * r], x0.x, fma(M[4 * r + 1], x1.x, fma(M[4 * r + 2], x2.x, M[4 * r + 3] * x3.x)));
-                y[r].y = fma(M[4 * r], x0.y, fma(M[4 * r + 1], x1.y, fma(M[4 * r + 2], x2.y, M[4 * r + 3] * x3.y)));
-            }
-            v[k] = y[0];
-            v[k1] = y[1];
-            v[k2] = y[2];
-            v[k3] = y[3];
-        }
-    }
-}
-
 // Shared-memory layout of a tile: element j lives at swz(j), which XORs the
 // low index bits with folds of the higher ones.  A warp's lanes differ in
 // three (complex128) or four (complex64) consecutive thread bits wherever the
@@ -529,105 +476,6 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
                 }
             break;
         }
-        case TOP_R1: {
-            const C c01 = coef[op.coef], c23 = coef[op.coef + 1];
-            switch (op.a) {
-#define QK_R1(S)                                        \
-    case S:                                             \
-        reg_r1<S>(v, c01, c23);                         \
-        if constexpr (NS == 2) reg_r1<S>(w, c01, c23);  \
-        break;
-            QK_R1(0) QK_R1(1) QK_R1(2) QK_R1(3) QK_R1(4)
-#undef QK_R1
-            }
-            break;
-        }
-        case TOP_R2: {
-            const C *m = coef + op.coef;
-            switch (op.a * 8 + op.b) {
-#define QK_R2(A, B)                                     \
-    case A * 8 + B:                                     \
-        reg_r2<A, B>(v, m);                             \
-        if constexpr (NS == 2) reg_r2<A, B>(w, m);      \
-        break;
-            QK_R2(0, 1) QK_R2(0, 2) QK_R2(0, 3) QK_R2(0, 4) QK_R2(1, 2)
-            QK_R2(1, 3) QK_R2(1, 4) QK_R2(2, 3) QK_R2(2, 4) QK_R2(3, 4)
-#undef QK_R2
-            }
-            break;
-        }
-        case TOP_PHASES: {
-            // the product of op.a factors (TOP_TERM records after this op,
-            // those with no register-slot qubit first): a factor whose qubits
-            // are both outside the register slots is the same for all of the
-            // thread's amplitudes and goes into cst; cst then rides on the
-            // first factor that varies over the register elements (or is
-            // applied alone), and each such factor takes one multiply per
-            // element
-            const int K = op.a;
-            C cst = mk<C>(1, 0);
-            bool folded = false;
-            for (int t = 1; t <= K; ++t) {
-                const TOp tm = prog[p + t];
-                const C *f = coef + tm.coef;
-                uint32_t ba, bb;
-                const int sa = code_slot_at(tm.a, tm.bits[0], base, tb, &ba);
-                const int sb = code_slot_at(tm.b, tm.bits[1], base, tb, &bb);
-                if (sa < 0 && sb < 0) {
-                    cst = cmul(cst, f[ba + 2 * bb]);
-                    continue;
-                }
-                if (sa >= 0 && sb >= 0) {
-                    C d0 = f[0], d1 = f[1], d2 = f[2], d3 = f[3];
-                    if (!folded) {
-                        d0 = cmul(d0, cst); d1 = cmul(d1, cst); d2 = cmul(d2, cst); d3 = cmul(d3, cst);
-                        folded = true;
-                    }
-                    switch (sa * 8 + sb) {
-#define QK_T2(A, B)                                                  \
-    case A * 8 + B:                                                  \
-        reg_diag2<A, B>(v, d0, d1, d2, d3);                          \
-        if constexpr (NS == 2) reg_diag2<A, B>(w, d0, d1, d2, d3);   \
-        break;                                                       \
-    case B * 8 + A:                                                  \
-        reg_diag2<B, A>(v, d0, d1, d2, d3);                          \
-        if constexpr (NS == 2) reg_diag2<B, A>(w, d0, d1, d2, d3);   \
-        break;
-                    QK_T2(0, 1) QK_T2(0, 2) QK_T2(0, 3) QK_T2(0, 4) QK_T2(1, 2)
-                    QK_T2(1, 3) QK_T2(1, 4) QK_T2(2, 3) QK_T2(2, 4) QK_T2(3, 4)
-#undef QK_T2
-                    }
-                } else {
-                    const int sl = sa >= 0 ? sa : sb;
-                    C p0 = sa >= 0 ? f[2 * bb] : f[ba], p1 = sa >= 0 ? f[1 + 2 * bb] : f[ba + 2];
-                    if (!folded) {
-                        p0 = cmul(p0, cst);
-                        p1 = cmul(p1, cst);
-                        folded = true;
-                    }
-                    switch (sl) {
-#define QK_T1(S)                                       \
-    case S:                                            \
-        reg_diag1<S>(v, p0, p1);                       \
-        if constexpr (NS == 2) reg_diag1<S>(w, p0, p1); \
-        break;
-                    QK_T1(0) QK_T1(1) QK_T1(2) QK_T1(3) QK_T1(4)
-#undef QK_T1
-                    }
-                }
-            }
-            if (!folded) {
-#pragma unroll
-                for (int k = 0; k < R; ++k) {
-                    v[k] = cmul(v[k], cst);
-                    if constexpr (NS == 2) w[k] = cmul(w[k], cst);
-                }
-            }
-            p += K;
-            break;
-        }
-        case TOP_TERM:
-            break;   // consumed by the TOP_PHASES before it
         case TOP_GRAD: {
             if constexpr (NS == 2) {
                 // summed over the warp in the state's precision, added to

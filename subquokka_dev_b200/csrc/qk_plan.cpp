@@ -79,8 +79,6 @@ size_t op_cost(const Op &op, int dtype) {
     const size_t c = dtype == QK_C128 ? 16 : 8;
     size_t ncoef = 4;
     if (op.kind == OP_DENSE2 || op.kind == OP_SWAP2 || op.kind == OP_CDENSE1) ncoef = 16;
-    else if (op.kind == OP_REAL2) ncoef = 8;
-    else if (op.kind == OP_REAL1) ncoef = 2;
     else if (op.kind == OP_PHASE1 || op.kind == OP_PHASE2) ncoef = 1;
     else if (op.kind == OP_CX) ncoef = 0;
     else if (op.kind == OP_GRAD) {
@@ -100,14 +98,6 @@ struct PassBuilder {
     // tile bits of a pass: false, as the ops in order need them; true, grown
     // ahead by the qubit that lets the most pending ops join
     bool lookahead = false;
-    // Diagonal ops commute with each other and with every op on other
-    // qubits, so the emitter holds them back (pend) until an op on one of
-    // their qubits, or the end of the pass, needs them applied, and then
-    // applies them together: three or more as one TOP_PHASES (one multiply
-    // per amplitude for the whole group), fewer one by one.
-    bool phase_tables = true;
-    std::vector<Op> pend = {};
-    std::vector<char> pend_q = {};
 
     // Emit a pass over tile bits B running ops[idx] (in order, dependencies
     // already satisfied with respect to everything outside idx).
@@ -121,8 +111,6 @@ struct PassBuilder {
         while (d.L < d.T && d.bpos[d.L] == d.L) ++d.L;
         std::vector<int> local(n, -1);
         for (int k = 0; k < d.T; ++k) local[B[k]] = k;
-        pend.clear();
-        pend_q.assign(n, 0);
         d.prog0 = (int)plan.ops.size();
         d.coef0 = (int)(plan.coef.size() / 2);
         d.grad0 = (int)plan.grad_params.size();
@@ -145,19 +133,8 @@ struct PassBuilder {
         size_t ndone = 0;
         bool mapped = false;
         size_t done_at_remap = (size_t)-1;
-        // an op touches the held-back diagonal ops when it acts on one of
-        // their qubits: emitting it applies them first
-        auto touches = [&](const Op &op) {
-            for (int k = 0; k < op.nq; ++k)
-                if (pend_q[op.q[k]]) return true;
-            return false;
-        };
         while (ndone < idx.size()) {
-            // ops that leave the held-back diagonals alone go first, so that
-            // one application covers as many of them as possible (with the
-            // list in layers: all of a layer's phases at once)
             bool progress = true;
-            bool allow_touch = !phase_tables;
             while (progress) {
                 progress = false;
                 for (size_t i = 0; i < idx.size(); ++i) {
@@ -168,25 +145,10 @@ struct PassBuilder {
                     for (int k = op_reg_first(op); k < op_reg_first(op) + op_reg_count(op); ++k)
                         ok = ok && in_regs(local[op.q[k]]);
                     if (!ok) continue;
-                    if (op_is_diagonal(op)) {
-                        pend.push_back(op);
-                        for (int k = 0; k < op.nq; ++k) pend_q[op.q[k]] = 1;
-                    } else {
-                        const bool touch = touches(op);
-                        if (touch && !allow_touch) continue;
-                        if (touch) flush(local, Q);
-                        emit(op, local, Q);
-                        allow_touch = !phase_tables;
-                    }
+                    emit(op, local, Q);
                     done[i] = 1;
                     ++ndone;
                     for (int k = 0; k < op.nq; ++k) ++head[op.q[k]];
-                    progress = true;
-                }
-                if (!progress && !allow_touch) {
-                    // nothing else is ready in the registers: a touching op
-                    // may go next (if none is ready either, re-map)
-                    allow_touch = true;
                     progress = true;
                 }
             }
@@ -206,10 +168,8 @@ struct PassBuilder {
                 for (int k = k0; k < k1; ++k)
                     if (std::find(nq.begin(), nq.end(), local[op.q[k]]) == nq.end()) nq.push_back(local[op.q[k]]);
             };
-            for (int pass_touch = phase_tables ? 0 : 1; pass_touch < 2; ++pass_touch)
-                for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
-                    if (!done[i] && ready(i) && op_reg_count(ops[idx[i]]) && (pass_touch || !touches(ops[idx[i]])))
-                        add(ops[idx[i]]);
+            for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
+                if (!done[i] && ready(i) && op_reg_count(ops[idx[i]])) add(ops[idx[i]]);
             for (size_t i = 0; i < idx.size() && (int)nq.size() < r; ++i)
                 if (!done[i] && op_reg_count(ops[idx[i]])) add(ops[idx[i]]);
             for (int b = 0; b < d.T && (int)nq.size() < r; ++b)
@@ -225,7 +185,6 @@ struct PassBuilder {
             ++plan.nremaps;
             mapped = true;
         }
-        flush(local, Q);
         d.nprog = (int)plan.ops.size() - d.prog0;
         d.ncoef = (int)(plan.coef.size() / 2) - d.coef0;
         d.ngrad = (int)plan.grad_params.size() - d.grad0;
@@ -239,108 +198,6 @@ struct PassBuilder {
 
     uint8_t code(int q, const std::vector<int> &local) {
         return local[q] >= 0 ? (uint8_t)local[q] : (uint8_t)(kOuterFlag | q);
-    }
-
-    // Value of a diagonal op at bit values (b0 of q[0], b1 of q[1]).
-    static void diag_value(const Op &op, int b0, int b1, double &re, double &im) {
-        re = 1;
-        im = 0;
-        switch (op.kind) {
-        case OP_PHASE1: if (b0) { re = op.m[0]; im = op.m[1]; } break;
-        case OP_DIAG1: re = op.m[2 * b0]; im = op.m[2 * b0 + 1]; break;
-        case OP_PHASE2: if (b0 && b1) { re = op.m[0]; im = op.m[1]; } break;
-        case OP_DIAG2: re = op.m[2 * (b0 + 2 * b1)]; im = op.m[2 * (b0 + 2 * b1) + 1]; break;
-        default: break;
-        }
-    }
-
-    // Apply the held-back diagonal ops: as they are when fewer than three,
-    // else merged into factors on qubit pairs (a two-qubit op starts a pair
-    // factor, or multiplies into the one on the same pair; a one-qubit op
-    // multiplies into a factor that holds its qubit, or starts its own) and
-    // emitted as one TOP_PHASES with a TOP_TERM per factor.
-    void flush(const std::vector<int> &local, const std::vector<int> &Q) {
-        if (pend.empty()) return;
-        std::vector<Op> ops_now;
-        ops_now.swap(pend);
-        std::fill(pend_q.begin(), pend_q.end(), 0);
-        if (!phase_tables || ops_now.size() < 2) {
-            for (const Op &op : ops_now) emit(op, local, Q);
-            return;
-        }
-        struct Term { int a, b; double f[8]; };
-        std::vector<Term> terms;
-        auto mul = [](double *f, double re, double im) {
-            const double x = f[0] * re - f[1] * im, y = f[0] * im + f[1] * re;
-            f[0] = x;
-            f[1] = y;
-        };
-        for (const Op &op : ops_now) {
-            if (op.nq != 2) continue;
-            Term *t = nullptr;
-            for (Term &x : terms)
-                if ((x.a == op.q[0] && x.b == op.q[1]) || (x.a == op.q[1] && x.b == op.q[0])) t = &x;
-            if (!t) {
-                terms.push_back(Term{op.q[0], op.q[1], {1, 0, 1, 0, 1, 0, 1, 0}});
-                t = &terms.back();
-            }
-            const bool same = t->a == op.q[0];
-            for (int i = 0; i < 4; ++i) {
-                double re, im;
-                const int b0 = same ? (i & 1) : (i >> 1), b1 = same ? (i >> 1) : (i & 1);
-                diag_value(op, b0, b1, re, im);
-                mul(t->f + 2 * i, re, im);
-            }
-        }
-        for (const Op &op : ops_now) {
-            if (op.nq != 1) continue;
-            const int q = op.q[0];
-            Term *t = nullptr;
-            for (Term &x : terms)
-                if (x.a == q || x.b == q) { t = &x; break; }
-            if (!t) {
-                terms.push_back(Term{q, -1, {1, 0, 1, 0, 1, 0, 1, 0}});
-                t = &terms.back();
-            }
-            for (int i = 0; i < 4; ++i) {
-                const int bit = t->a == q ? (i & 1) : (i >> 1);
-                double re, im;
-                diag_value(op, bit, 0, re, im);
-                mul(t->f + 2 * i, re, im);
-            }
-        }
-        auto slot_of = [&](uint8_t c) -> uint8_t {
-            if (c == kNoQubit || (c & kOuterFlag)) return kNoSlot;
-            const auto it = std::find(Q.begin(), Q.end(), (int)c);
-            return it == Q.end() ? kNoSlot : (uint8_t)(it - Q.begin());
-        };
-        // factors with no register-slot qubit first: the kernel folds their
-        // product into the first factor that has one
-        auto is_slot = [&](int q) { return q >= 0 && local[q] >= 0 && slot_of((uint8_t)local[q]) != kNoSlot; };
-        std::stable_partition(terms.begin(), terms.end(),
-                              [&](const Term &x) { return !is_slot(x.a) && !is_slot(x.b); });
-        for (size_t t0 = 0; t0 < terms.size(); t0 += 255) {
-            const size_t nt = std::min<size_t>(255, terms.size() - t0);
-            TOp h;
-            std::memset(&h, 0, sizeof h);
-            h.kind = TOP_PHASES;
-            h.a = (uint8_t)nt;
-            h.coef = (uint32_t)(plan.coef.size() / 2);
-            plan.ops.push_back(h);
-            for (size_t j = t0; j < t0 + nt; ++j) {
-                const Term &x = terms[j];
-                TOp t;
-                std::memset(&t, 0, sizeof t);
-                t.kind = TOP_TERM;
-                t.a = code(x.a, local);
-                t.b = x.b < 0 ? kNoQubit : code(x.b, local);
-                t.bits[0] = slot_of(t.a);
-                t.bits[1] = slot_of(t.b);
-                t.coef = (uint32_t)(plan.coef.size() / 2);
-                for (int i = 0; i < 4; ++i) push_c(plan, x.f[2 * i], x.f[2 * i + 1]);
-                plan.ops.push_back(t);
-            }
-        }
     }
 
     void emit(const Op &op, const std::vector<int> &local, const std::vector<int> &Q) {
@@ -407,30 +264,6 @@ struct PassBuilder {
                         push_c(plan, m[2 * k], m[2 * k + 1]);
                     }
             }
-            break;
-        }
-        case OP_REAL1:
-            t.kind = TOP_R1;
-            t.a = (uint8_t)slot(op.q[0]);
-            push_c(plan, op.m[0], op.m[1]);
-            push_c(plan, op.m[2], op.m[3]);
-            break;
-        case OP_REAL2: {
-            int sa = slot(op.q[0]), sb = slot(op.q[1]);
-            t.kind = TOP_R2;
-            double m[16];
-            if (sa < sb) {
-                std::memcpy(m, op.m, sizeof m);
-            } else {
-                // index bit 0 must be the lower slot: swap the two index bits
-                std::swap(sa, sb);
-                auto sw = [](int i) { return ((i & 1) << 1) | ((i >> 1) & 1); };
-                for (int i = 0; i < 4; ++i)
-                    for (int j = 0; j < 4; ++j) m[4 * sw(i) + sw(j)] = op.m[4 * i + j];
-            }
-            t.a = (uint8_t)sa;
-            t.b = (uint8_t)sb;
-            for (int k = 0; k < 8; ++k) push_c(plan, m[2 * k], m[2 * k + 1]);
             break;
         }
         case OP_CX:
@@ -719,7 +552,6 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
         relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant >= 4);
         merge_one_qubit_runs(ops, n);
         absorb_into_two_qubit_ops(ops, n);
-        split_real(ops);
         if (variant % 2) asap_order(ops, n);
         HostPlan hp;
         hp.n = n;

@@ -6,7 +6,6 @@
 //   no longer split runs of one-qubit ops;
 // - relabel_perms: VSWAPs (and optionally SWAPs) as renamings of qubits.
 #include <algorithm>
-#include <cmath>
 #include <array>
 #include <cstring>
 #include <utility>
@@ -444,113 +443,4 @@ void relabel_perms(std::vector<Op> &ops, int n, int L, int max_bits, int max_pai
     ops.swap(out);
 }
 
-
-// Factor a d x d complex matrix (row-major (re, im)) as D_L R D_R with D_L,
-// D_R diagonal of unit phases and R real: phases are assigned along a
-// spanning forest of the nonzero entries (rows and columns as the two sides
-// of a bipartite graph), R = D_L^-1 M D_R^-1, and the factorisation is kept
-// only if every entry of R is real to 1e-14 of the largest entry.  Every
-// unitary factors this way (in U(2), D_L R D_R with R a rotation; two-qubit
-// ops that are a diagonal times a tensor product of one-qubit ops too), and
-// so do real matrices like the reference's H (not quite unitary, with its
-// truncated constant), which come back unchanged.
-static bool real_factor(const double *m, int d, double *dl, double *r, double *dr) {
-    double big = 0;
-    for (int k = 0; k < d * d; ++k) big = std::max(big, std::hypot(m[2 * k], m[2 * k + 1]));
-    if (big == 0) return false;
-    const double tiny = 1e-300;
-    std::vector<int> rs(d, 0), cs(d, 0);   // 1 = phase assigned
-    for (int k = 0; k < d; ++k) {
-        dl[2 * k] = dr[2 * k] = 1;
-        dl[2 * k + 1] = dr[2 * k + 1] = 0;
-    }
-    auto nz = [&](int i, int j) { return std::hypot(m[2 * (d * i + j)], m[2 * (d * i + j) + 1]) > tiny; };
-    for (int start = 0; start < d; ++start) {
-        if (rs[start]) continue;
-        bool any = false;
-        for (int j = 0; j < d; ++j) any = any || nz(start, j);
-        if (!any) continue;
-        rs[start] = 1;   // phase 1 for the first row of a component
-        bool grew = true;
-        while (grew) {
-            grew = false;
-            for (int i = 0; i < d; ++i)
-                for (int j = 0; j < d; ++j) {
-                    if (!nz(i, j) || rs[i] == cs[j]) continue;
-                    const double mr = m[2 * (d * i + j)], mi = m[2 * (d * i + j) + 1], a = std::hypot(mr, mi);
-                    const double wr = mr / a, wi = mi / a;   // unit phase of the entry
-                    if (rs[i]) {   // mu_j = w / lambda_i
-                        const double lr = dl[2 * i], li = dl[2 * i + 1];
-                        dr[2 * j] = wr * lr + wi * li;
-                        dr[2 * j + 1] = wi * lr - wr * li;
-                        cs[j] = 1;
-                    } else {       // lambda_i = w / mu_j
-                        const double ur = dr[2 * j], ui = dr[2 * j + 1];
-                        dl[2 * i] = wr * ur + wi * ui;
-                        dl[2 * i + 1] = wi * ur - wr * ui;
-                        rs[i] = 1;
-                    }
-                    grew = true;
-                }
-        }
-    }
-    for (int i = 0; i < d; ++i)
-        for (int j = 0; j < d; ++j) {
-            // R_ij = M_ij conj(lambda_i) conj(mu_j)
-            const double mr = m[2 * (d * i + j)], mi = m[2 * (d * i + j) + 1];
-            const double pr = dl[2 * i] * dr[2 * j] - dl[2 * i + 1] * dr[2 * j + 1];
-            const double pi = dl[2 * i] * dr[2 * j + 1] + dl[2 * i + 1] * dr[2 * j];
-            const double re = mr * pr + mi * pi, im = mi * pr - mr * pi;
-            if (std::fabs(im) > 1e-14 * big) return false;
-            r[d * i + j] = re;
-        }
-    return true;
-}
-
-static bool unit_phases(const double *p, int d) {
-    for (int k = 0; k < d; ++k)
-        if (std::fabs(p[2 * k] - 1) > 1e-16 || std::fabs(p[2 * k + 1]) > 1e-16) return false;
-    return true;
-}
-
-// Dense ops become D_R, a real op, D_L (diagonal ops around a real one).  A
-// real one-qubit op costs two real multiply-adds per output component where a
-// complex one costs four, and the diagonal ops cost little once the pass
-// emitter merges the many of a layer into one phase table (TOP_PHASES).
-// OP_DENSE1 -> OP_REAL1, OP_DENSE2 -> OP_REAL2; ops that do not factor stay.
-void split_real(std::vector<Op> &ops) {
-    std::vector<Op> out;
-    out.reserve(3 * ops.size());
-    for (const Op &op : ops) {
-        if (op.kind != OP_DENSE1 && op.kind != OP_DENSE2) {
-            out.push_back(op);
-            continue;
-        }
-        const int d = op.kind == OP_DENSE1 ? 2 : 4;
-        double dl[8], r[16], dr[8];
-        if (!real_factor(op.m, d, dl, r, dr)) {
-            out.push_back(op);
-            continue;
-        }
-        auto diag = [&](const double *p) {
-            Op g;
-            std::memset(&g, 0, sizeof g);
-            g.kind = d == 2 ? OP_DIAG1 : OP_DIAG2;
-            g.nq = op.nq;
-            for (int k = 0; k < op.nq; ++k) g.q[k] = op.q[k];
-            std::memcpy(g.m, p, sizeof(double) * 2 * d);
-            return g;
-        };
-        if (!unit_phases(dr, d)) out.push_back(diag(dr));
-        Op x;
-        std::memset(&x, 0, sizeof x);
-        x.kind = d == 2 ? OP_REAL1 : OP_REAL2;
-        x.nq = op.nq;
-        for (int k = 0; k < op.nq; ++k) x.q[k] = op.q[k];
-        std::memcpy(x.m, r, sizeof(double) * d * d);
-        out.push_back(x);
-        if (!unit_phases(dl, d)) out.push_back(diag(dl));
-    }
-    ops.swap(out);
-}
 }  // namespace qk

@@ -21,8 +21,6 @@
 // States agree within 1e-12; gradients within 1e-12, or 1e-9 for circuits
 // with H (the reference's H constant is 1.1e-11 off unitary, and gradient
 // ops move past gates on other qubits).  Exit status 0 on success.
-#include <algorithm>
-
 #include "dense_sim.h"
 
 using namespace dense_sim;
@@ -156,72 +154,6 @@ void emulate(const HostPlan &hp, State &psi, State *lam, std::vector<double> &g)
                                     x[si][j] *= coef(op, 0);
                             }
                     break;
-                case qk::TOP_R1: {
-                    // real 2x2: coefficients (a, b), (c, d)
-                    const double a = coef(op, 0).real(), b = coef(op, 0).imag(), c = coef(op, 1).real(),
-                                 dd = coef(op, 1).imag();
-                    for (int si = 0; si < 2; ++si)
-                        if (states[si])
-                            pairs(Q.at(op.a), [&](uint64_t j0, uint64_t j1) {
-                                const cd u = x[si][j0], v = x[si][j1];
-                                x[si][j0] = a * u + b * v;
-                                x[si][j1] = c * u + dd * v;
-                            });
-                    break;
-                }
-                case qk::TOP_R2: {
-                    // real 4x4, the 16 reals two to a coefficient
-                    double M[16];
-                    for (int k = 0; k < 8; ++k) {
-                        M[2 * k] = coef(op, k).real();
-                        M[2 * k + 1] = coef(op, k).imag();
-                    }
-                    const int ta = Q.at(op.a), tb = Q.at(op.b);
-                    for (int si = 0; si < 2; ++si)
-                        if (states[si])
-                            for (uint64_t j = 0; j < tn; ++j) {
-                                if (((j >> ta) & 1) || ((j >> tb) & 1)) continue;
-                                const uint64_t idx[4] = {j, j | (1ull << ta), j | (1ull << tb),
-                                                         j | (1ull << ta) | (1ull << tb)};
-                                cd in[4], out[4];
-                                for (int k = 0; k < 4; ++k) in[k] = x[si][idx[k]];
-                                for (int r = 0; r < 4; ++r) {
-                                    out[r] = 0;
-                                    for (int k = 0; k < 4; ++k) out[r] += M[4 * r + k] * in[k];
-                                }
-                                for (int k = 0; k < 4; ++k) x[si][idx[k]] = out[k];
-                            }
-                    break;
-                }
-                case qk::TOP_PHASES: {
-                    // product of the op.a TOP_TERM factors that follow; every
-                    // term's slots must name the register slot of its code
-                    for (int t = 1; t <= op.a; ++t) {
-                        const TOp &tm = hp.ops.at((size_t)pi + t);
-                        if (tm.kind != qk::TOP_TERM) {
-                            std::fprintf(stderr, "TOP_PHASES followed by op %d\n", tm.kind);
-                            std::exit(2);
-                        }
-                        for (int e = 0; e < 2; ++e) {
-                            const uint8_t c = e ? tm.b : tm.a, sl = tm.bits[e];
-                            const bool local = c != qk::kNoQubit && !(c & qk::kOuterFlag);
-                            const auto it = local ? std::find(Q.begin(), Q.end(), (int)c) : Q.end();
-                            const uint8_t want = it == Q.end() ? qk::kNoSlot : (uint8_t)(it - Q.begin());
-                            if (sl != want) {
-                                std::fprintf(stderr, "TOP_TERM slot %d, register mapping says %d\n", sl, want);
-                                std::exit(2);
-                            }
-                        }
-                        for (int si = 0; si < 2; ++si)
-                            if (states[si])
-                                for (uint64_t j = 0; j < tn; ++j) {
-                                    const int ba = bit_of(tm.a, j, base), bb = bit_of(tm.b, j, base);
-                                    x[si][j] *= coef(tm, (ba < 0 ? 0 : ba) + 2 * (bb < 0 ? 0 : bb));
-                                }
-                    }
-                    pi += op.a;
-                    break;
-                }
                 case qk::TOP_GRAD: {
                     const int gen = op.b;
                     const int tb = Q.at(op.a);

@@ -11,10 +11,8 @@ def test_random30_is_far_fewer_passes_than_gates():
     c = circuits.random_u3_cz(30, 20, 2030)
     passes, ops, remaps = Plan(c, 30, "c128").stats()
     assert c.ngates == 890
-    # U3 pairs fold into the CZ after them as one real 4x4 between phase
-    # factors; the phases of a layer are applied together (one TOP_PHASES
-    # and a 16-byte TOP_TERM record per factor in the program)
-    assert passes <= 24 and ops <= 2 * c.ngates and remaps < ops // 4
+    # U3 pairs fold into the CZ after them: fewer program ops than gates
+    assert passes <= 45 and ops <= c.ngates // 2 and remaps < ops
 
 
 def test_diagonal_gates_join_any_pass():
@@ -36,9 +34,9 @@ def test_program_op_reductions():
     c, _ = pc.bind(np.random.default_rng(26).uniform(-np.pi, np.pi, pc.nparams))
     assert c.ngates == 924
     passes, ops, _ = Plan(c, 26, "c128").stats()
-    assert ops <= 420 and passes <= 24
+    assert ops <= 400 and passes <= 30
     brick = circuits.random_u3_cz(30, 20, 2030)
-    assert Plan(brick, 30, "c64").stats()[0] <= 22
+    assert Plan(brick, 30, "c64").stats()[1] <= 420
 
 
 def test_vswap_is_a_relabelling():
