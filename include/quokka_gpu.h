@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define QK_ABI_VERSION 2   /* 2: qk_config.init_file */
+#define QK_ABI_VERSION 3   /* 2: qk_config.init_file; 3: qk_config.device_qbit */
 #define QK_MAX_TARGETS 12
 
 /* Status codes.  The reference reports errors by printing to cerr and calling
@@ -106,6 +106,11 @@ typedef struct qk_config {
     char init_file[256];      /* init_file, default "": a state file
                                  (qk_sv_load) to start from instead of
                                  |0...0>                                     */
+    int32_t device_qbit;      /* device_qbit, default 0: with runner_type IO
+                                 or DirectIO the state lives in host memory
+                                 (qk_hsv) and the GPU takes chunks of
+                                 2^device_qbit amplitudes; 0 = the largest
+                                 that fits three chunks in free HBM         */
 } qk_config;
 
 typedef struct qk_circuit qk_circuit;   /* parsed gate list (+ group sizes) */

@@ -17,7 +17,7 @@ QK_MAX_TARGETS = 12
 QK_C128, QK_C64 = 0, 1
 
 # qk_gate_kind
-ABI_VERSION = 2   # QK_ABI_VERSION of include/quokka_gpu.h that QkGate / QkConfig below mirror
+ABI_VERSION = 3   # QK_ABI_VERSION of include/quokka_gpu.h that QkGate / QkConfig below mirror
 
 GATE_KINDS = {
     "H": 1, "X": 2, "Y": 3, "Z": 4, "P": 5, "RX": 6, "RY": 7, "RZ": 8,
@@ -56,6 +56,7 @@ class QkConfig(ctypes.Structure):
         ("runner_type", c_char * 32),
         ("dump_file", c_char * 256),
         ("init_file", c_char * 256),
+        ("device_qbit", c_int32),
     ]
 
 

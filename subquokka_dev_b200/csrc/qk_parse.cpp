@@ -467,6 +467,9 @@ int qk_config_load(const char *ini_path, qk_config *out) {
     c.fuse_width = (int32_t)ini.get_int(S, "fuse_width", 0);
     c.dump_binary = lower(ini.get(S, "dump_format", "txt")) == "bin";
     std::snprintf(c.init_file, sizeof c.init_file, "%s", ini.get(S, "init_file", "").c_str());
+    c.device_qbit = (int32_t)ini.get_int(S, "device_qbit", 0);
+    if (c.device_qbit < 0 || c.device_qbit > c.total_qbit - c.mpi_qbit)
+        return fail(QK_ERR_ARG, "device_qbit must be in [0, %d], got %d", c.total_qbit - c.mpi_qbit, c.device_qbit);
     // the reference's asserts (src/simulator.cpp:98-99, :152)
     const int n_local = c.total_qbit - c.mpi_qbit;
     if (c.chunk_qbit < 1) return fail(QK_ERR_ARG, "chunk_qbit must be >= 1 (got %d)", c.chunk_qbit);

@@ -29,13 +29,13 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) <= set(_lib.PROTOTYPES), set(names) - set(_lib.PROTOTYPES)
-    assert lib.qk_abi_version() == 2
+    assert lib.qk_abi_version() == 3
 
 
 def test_struct_layouts_match_header():
     import ctypes
     assert ctypes.sizeof(_lib.QkGate) == 4 + 4 + 4 * 12 + 8 + 8 * 32
-    assert ctypes.sizeof(_lib.QkConfig) == 10 * 4 + 32 + 256 + 256
+    assert ctypes.sizeof(_lib.QkConfig) == 10 * 4 + 32 + 256 + 256 + 4
 
 
 def write(tmp_path, name, text):
@@ -75,6 +75,14 @@ def test_ini_reference_asserts_become_errors(tmp_path, body, code):
     with pytest.raises(sq.QkError) as e:
         Config(write(tmp_path, "c.ini", body))
     assert e.value.code == code
+
+
+def test_ini_device_qbit_key(tmp_path):
+    # engine key for the host-resident runner (runner_type IO / DirectIO)
+    assert Config(write(tmp_path, "d.ini", "[system]\ntotal_qbit=20\nchunk_qbit=4\n")).device_qbit == 0
+    assert Config(write(tmp_path, "e.ini", "[system]\ntotal_qbit=20\nchunk_qbit=4\ndevice_qbit=16\n")).device_qbit == 16
+    with pytest.raises(sq.QkError):
+        Config(write(tmp_path, "f.ini", "[system]\ntotal_qbit=20\nchunk_qbit=4\ndevice_qbit=21\n"))
 
 
 def test_ini_missing_file():
@@ -151,7 +159,7 @@ def test_cli_argument_errors():
 
 
 def test_cli_rejects_other_runner_types(tmp_path):
-    ini = write(tmp_path, "d.ini", "[system]\ntotal_qbit=4\nchunk_qbit=2\nrunner_type=IO\n")
+    ini = write(tmp_path, "d.ini", "[system]\ntotal_qbit=4\nchunk_qbit=2\nrunner_type=RDMA\n")
     cir = write(tmp_path, "c.txt", "H 0\n")
     r = subprocess.run([CLI, "-i", ini, "-c", cir], capture_output=True, text=True)
     assert r.returncode == 1 and "runner not found" in r.stderr

@@ -2,6 +2,9 @@
 gates on the GPU chunk by chunk.  Against the FP64 oracle and the in-HBM
 per-gate path, for chunks much smaller than the state (many chunks per
 segment, several segments, gathers with strides)."""
+import os
+import subprocess
+
 import numpy as np
 import pytest
 
@@ -50,3 +53,29 @@ def test_host_state_reset_and_empty_circuit():
         h.apply(Circuit([]))
         v = h.view()
         assert v[0] == 1 and np.count_nonzero(v) == 1
+
+
+CLI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "subquokka_dev_b200", "bin",
+                   "quokka")
+
+
+@pytest.mark.parametrize("name,dq,precision,tol", [("qft12", 8, "c128", 1e-12), ("sub12", 9, "c128", 1e-12),
+                                                   ("rand10", 7, "c128", 1e-12), ("qft21", 17, "c128", 1e-12),
+                                                   ("qft12", 9, "c64", 2e-6)])
+def test_cli_io_runner_on_host_state(tmp_path, name, dq, precision, tol):
+    """runner_type=IO: the reference's out-of-core runner's slot, here the
+    state in host memory and 2^device_qbit-amplitude chunks on the GPU; the
+    reference's golden final states (flat and subcircuit files)."""
+    import golden_util as gu
+    rec = gu.load(name)
+    gu.initial_state(rec).astype(np.complex128).tofile(tmp_path / "init.bin")
+    ini = tmp_path / "io.ini"
+    ini.write_text(f"[system]\ntotal_qbit={rec['n']}\nfile_qbit=0\nchunk_qbit=4\nrunner_type=IO\n"
+                   f"is_subcircuit={rec['is_subcircuit']}\ninit_file={tmp_path}/init.bin\ndevice_qbit={dq}\n"
+                   f"precision={precision}\ndump_file={tmp_path}/state.bin\ndump_format=bin\n")
+    (tmp_path / "c.txt").write_text(rec["circuit"])
+    r = subprocess.run([CLI, "-i", str(ini), "-c", str(tmp_path / "c.txt")], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "IO Mode" in r.stdout
+    assert gu.compare(rec, np.fromfile(tmp_path / "state.bin", dtype=np.complex128)) <= tol
