@@ -167,3 +167,27 @@ def test_workspace_reuse_and_release(fused):
         assert abs(ev - ref[0]) < 1e-12
         assert np.abs(g - ref[1]).max() < 1e-11
         assert drift < 1e-12
+
+
+def test_last_sweep_reports_device_time_and_traffic():
+    """qk_sv_last_sweep: CUDA-event time of the sweep and, for the fused form,
+    its algorithmic bytes = 2S per forward pass + 4S per two-state pass + the
+    H application, reductions and checkpoint copies."""
+    from subquokka_dev_b200 import QkError, last_sweep
+    n = 14
+    pc = hea_template(n, 3)
+    rng = np.random.default_rng(5)
+    params = rng.uniform(-np.pi, np.pi, pc.nparams)
+    terms = zz_x_hamiltonian(n, rng.standard_normal(n - 1), rng.standard_normal(n))
+    circ, idx = pc.bind(params)
+    with StateVector(n, "c64") as sv:
+        with pytest.raises(QkError):
+            last_sweep(sv)                       # nothing has run yet
+        adjoint_grad(sv, circ, idx, pc.nparams, terms, 0, True)
+        st = last_sweep(sv)
+        S = 8 << n
+        assert st["device_ms"] > 0 and st["forward_passes"] > 0 and st["backward_passes"] > 0
+        assert st["alg_bytes"] >= 2 * S * st["forward_passes"] + 4 * S * st["backward_passes"]
+        adjoint_grad(sv, circ, idx, pc.nparams, terms, 0, False)
+        st = last_sweep(sv)
+        assert st["alg_bytes"] == 0 and st["forward_passes"] == circ.ngates

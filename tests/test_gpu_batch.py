@@ -92,3 +92,13 @@ def test_sharded_batch_shards_give_the_whole_batch():
     assert np.abs(got_ev - ev).max() <= 1e-12
     for c in range(len(items)):
         assert np.abs(got_g[c] - grads[c]).max() <= 1e-12
+
+
+def test_batch_timing_reports_device_time_and_bytes():
+    items = circuits.variational_batch(4, 53, qmin=8, qmax=10, lmin=1, lmax=2)
+    b = Batch(items, "c64")
+    b.run()
+    ms, nbytes = b.timing()
+    # at least a forward and a backward pass, reset, H and drift per circuit
+    assert ms > 0 and nbytes >= sum(10 * (8 << pc.n) for pc, _, _ in items)
+    b.close()
