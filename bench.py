@@ -623,6 +623,35 @@ def host_state_workload(n, L):
     return res
 
 
+def sharded_state(world, layers):
+    """One state over all ranks (ShardedStateVector): the random circuit on
+    30 + log2(N) qubits, 2^30 complex128 amplitudes a rank (weak scaling),
+    exchanges by NCCL all-to-all; the slowest rank's device time."""
+    import torch
+    import torch.distributed as dist
+    from subquokka_dev_b200 import circuits
+    from subquokka_dev_b200.sharding import ShardedStateVector
+    g = world.bit_length() - 1
+    if world & (world - 1):
+        return {"skipped": "the number of ranks is not a power of two"}
+    n = 30 + g
+    circ = circuits.random_u3_cz(n, layers, SEED)
+    sv = ShardedStateVector(n, "c128")
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sv.apply(circ)
+    e1.record()
+    torch.cuda.synchronize()
+    worst = max_over_ranks(e0.elapsed_time(e1), world)
+    out = {"qubits": n, "ranks": world, "scaling": "weak", "amplitudes_per_rank": 1 << 30, "gates": circ.ngates,
+           "exchanges": sv.exchanges, "max_rank_ms": worst, "gates_per_s": circ.ngates / (worst / 1e3),
+           "timed": "one apply: host planning of each segment, fused passes, all-to-all exchanges"}
+    sv.close()
+    return out
+
+
 def our_arm(args, rank, world):
     import numpy as np
     import torch
@@ -696,9 +725,10 @@ def our_arm(args, rank, world):
     launches = args.steps * (circ.ngates + 1)
     variants = {} if args.no_fused else fused_variants(args, circ, sv, ms_per_step, alg)
     extra = {} if (args.no_extra or rank != 0) else None
-    sharded = None
+    sharded = sharded_st = None
     if world > 1 and not args.no_extra:
         sharded = sharded_batch(world)   # every rank takes part
+        sharded_st = sharded_state(world, args.layers)
 
     # end to end through the public API: host gate records in, final state out to pinned host memory
     e2e = None
@@ -746,6 +776,8 @@ def our_arm(args, rank, world):
                 "gpu_launches": launches, "fused": variants, "workloads": extra}
         if sharded is not None:
             line["batch256_sharded"] = sharded
+        if sharded_st is not None:
+            line["random_sharded_state"] = sharded_st
         # last, so that a reader of the line's tail sees every target at once
         line["summary"] = summarize(line, peak)
         print(json.dumps(line))
