@@ -261,15 +261,14 @@ class ShardedStateVector:
             dist.all_to_all_single(self._real(y), self._real(x), splits, splits, group=self.group)
             self.backend.swap_in(self.shards[r])
         else:
-            new = {}
+            # every rank hosted here: the same blocks moved by device copies
             for r in self.ranks:
                 y = self.backend.scratch(self.shards[r])
                 block = y.numel() // nb
+                v = sum(((r >> b) & 1) << i for i, b in enumerate(G))   # the block each source sends to r
                 for u in range(nb):
-                    s = (r & ~gmask) | _deposit(u, G)        # the source rank
-                    v = sum(((r >> b) & 1) << i for i, b in enumerate(G))   # the block s sends to r
+                    s = (r & ~gmask) | _deposit(u, G)        # the source rank of block u
                     y[u * block:(u + 1) * block].copy_(self.backend.tensor(self.shards[s])[v * block:(v + 1) * block])
-                new[r] = y
             for r in self.ranks:
                 self.backend.swap_in(self.shards[r])
 
@@ -311,6 +310,8 @@ class EngineShards:
     def __init__(self, dtype="c128", fused: bool = True):
         self.dtype = dtype
         self.fused = fused
+        self._plan = None
+        self._plan_for = None
 
     def zero(self, m: int, first: bool):
         from .engine import StateVector
@@ -335,14 +336,20 @@ class EngineShards:
         from .engine import Plan
         if not circ.ngates:
             return
-        if self.fused:
-            p = Plan(circ, m, self.dtype)
-            p.apply(sh["cur"])
-            p.close()
-        else:
+        if not self.fused:
             sh["cur"].apply(circ)
+            return
+        # the ranks hosted here run the same gate list: one plan for all of them
+        if self._plan_for is not circ:
+            if self._plan is not None:
+                self._plan.close()
+            self._plan, self._plan_for = Plan(circ, m, self.dtype), circ
+        self._plan.apply(sh["cur"])
 
     def close(self, sh):
         for key in ("cur", "other"):
             if sh[key] is not None:
                 sh[key].close()
+        if self._plan is not None:
+            self._plan.close()
+            self._plan, self._plan_for = None, None
