@@ -308,7 +308,8 @@ def fused_variants(args, circ, exact, plain_ms, alg):
     n = args.qubits
     from subquokka_dev_b200 import chunk_groups
     sub = chunk_groups(circ, n, 12)   # the circuit as a subcircuit file, 12-qubit chunks
-    for key, dtype, fw in (("c128", "c128", 0), ("c64", "c64", 0), ("c64_tensor_core", "c64", 6),
+    for key, dtype, fw in (("c128", "c128", 0), ("c128_tensor_core", "c128", 6), ("c64", "c64", 0),
+                           ("c64_tensor_core", "c64", 6),
                            ("c64_tensor_core_width5", "c64", 5), ("c128_subcircuit_file", "c128", -1),
                            ("c64_subcircuit_file", "c64", -1), ("c64_tensor_core_subcircuit_file", "c64", -6)):
         plan = (Plan(sub, n, dtype, groups=True, fuse_width=-fw if fw < -1 else 0) if fw < 0
@@ -792,7 +793,8 @@ def summarize(line, peak):
     out = {"plain_c128_s": r(line["circuit_seconds"]), "plain_c128_hbm_frac": r(line["hbm_frac_of_peak"], 3),
            "plain_c128_kernel_frac": r(line["roofline"]["frac"], 3)}
     f = line.get("fused") or {}
-    for key, name in (("c64_tensor_core", "fused_c64_tc"), ("c128", "fused_c128"), ("c64", "fused_c64")):
+    for key, name in (("c64_tensor_core", "fused_c64_tc"), ("c128_tensor_core", "fused_c128_tc"),
+                      ("c128", "fused_c128"), ("c64", "fused_c64")):
         if key in f:
             v = f[key]
             out[name] = {"s": r(v["ms_per_circuit"] / 1e3), "x_vs_plain": r(v["speedup_vs_plain_c128"], 3),

@@ -1,0 +1,458 @@
+// Dense fused blocks on the 5th-generation tensor cores, complex128 states.
+//
+// The block is the same 64 x 64 complex unitary U on six qubits as in the
+// complex64 kernel (qk_dense_tc.cu), applied to supertiles of 64 x 64
+// amplitudes (the block's six qubits x the lowest six other state bits) as
+// the real contraction
+//
+//   D[m][n] = sum_k W[m][k] S[n][k]          m, k < 128, n < 64
+//   W[2i'+a][2i+c] = [[Ur, -Ui], [Ui, Ur]][a][c] (i', i)
+//   S[n][2i+c]     = (re, im)_c X[i][n],     X'[i'][n] = D[2i'][n] + i D[2i'+1][n]
+//
+// in exact integer arithmetic on the int8 tensor cores (tcgen05.mma
+// kind::i8, int32 accumulators), an Ozaki-type split:
+//
+//   - every row of W and every row n of S is scaled by a power of two to a
+//     55-bit integer v (|v| < 2^54): W rows on the host, rounded, as seven
+//     balanced digits in [-128, 127]; state rows on the device, truncated,
+//     as the seven low bytes of v in two's complement (six unsigned digits
+//     and a signed top digit in [-64, 63]);
+//   - sum_k v_w v_s = sum_(i, j) 2^(8 (i + j)) sum_k w_i s_j.  The 28 digit
+//     products with i + j >= 6 are computed; the dropped ones lie below
+//     2^-50 of the result.  Products of one weight d = i + j add up in one
+//     int32 accumulator (|sum| <= 7 x 128 x 128 x 255 < 2^25);
+//   - the seven accumulators of a supertile are combined in FP64 and scaled
+//     back (2^(e_w - 1028) 2^(e_s - 1028), e = the row's largest biased
+//     exponent).  Rows whose largest entry is below 2^-1017 come out as zero.
+//
+// The result matches FP64 arithmetic to about 2^-50 relative per block.
+//
+// Operands and memory:
+//   - W's digit planes are the A operand in tensor memory (lane m = row m,
+//     four digits of consecutive k per 32-bit column; plane i at columns
+//     32 i .. 32 i + 31), loaded once per CTA with tcgen05.st.
+//   - The state's digit planes are the B operand in shared memory (N = 64
+//     rows n, K-major, 128-byte swizzle: 8 KiB a plane, seven planes).
+//   - Accumulators D[m][n]: four slots of 64 columns (a ring over the seven
+//     weights of consecutive supertiles), TMEM columns 256 .. 511.
+//   - Raw supertiles (64 KiB of complex128) are staged in shared memory by
+//     cp.async, two buffers, so that the load of supertile s + 2 runs while
+//     s and s + 1 are processed; their 16-byte slots are XOR-swizzled so that
+//     both the coalesced copy and the per-row reads are free of bank
+//     conflicts.
+//
+// Roles (16 data warps + 1 issuer warp): per supertile the data warps split
+// the staged amplitudes into digit planes (thread = row n, block indices
+// 8 g .. 8 g + 7), hand them to the issuer, refill the staging buffer, then
+// drain the seven accumulators as their MMAs complete (thread = TMEM lane m,
+// 16 columns n), combine them in FP64 and store the supertile.  One elected
+// thread issues the 28 x 4 MMAs (M128 N64 K32) of a supertile and commits
+// each weight's accumulator to an mbarrier.  Every wait is bounded: a wait
+// that runs out sets an error code (1), the data warps agree on stopping at
+// their next barrier, and the issuer releases the TMEM only after its last
+// MMAs have completed (3 if that wait runs out).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "qk_device.h"
+#include "qk_internal.h"
+#include "qk_pass_device.cuh"
+#include "qk_tc_device.cuh"
+
+namespace qk {
+
+constexpr int kI8DataWarps = 16;
+constexpr int kI8DataThreads = 32 * kI8DataWarps;
+constexpr int kI8Threads = kI8DataThreads + 32;             // + one MMA-issuer warp
+constexpr uint32_t kI8PlaneBytes = 64u * 128u;              // one digit plane of the state operand
+constexpr uint32_t kI8BufBytes = kI8Digits * kI8PlaneBytes; // the seven planes of one supertile
+constexpr uint32_t kI8Smem = 2u * kI8BufBytes;              // two supertiles: 112 KiB
+constexpr uint32_t kI8WCols = 32u * kI8Digits;              // W digit planes, TMEM columns 0 .. 223
+constexpr uint32_t kI8AccCol = 256;                         // accumulator slot r at 256 + 64 r
+constexpr int kI8Slots = 4;
+constexpr int kI8LowWeight = 6;                             // digit products of weight i + j >= this
+constexpr int kI8Weights = 2 * (kI8Digits - 1) + 1 - kI8LowWeight;
+constexpr uint32_t kI8TmemCols = 512;
+static_assert(kI8WCols <= kI8AccCol, "digit planes overlap the accumulators");
+
+// kind::i8, D = S32, A = W digits (signed), B = state digits (unsigned for
+// planes 0-5, signed for the top plane), both K-major, M = 128, N = 64
+constexpr uint32_t kI8IdescU = (2u << 4) | (1u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kI8IdescS = kI8IdescU | (1u << 10);
+
+// 4 x 4 byte transpose: out[j] = byte j of in[0], in[1], in[2], in[3]
+__device__ __forceinline__ void bytes4x4(const uint32_t (&in)[4], uint32_t (&out)[4]) {
+    const uint32_t t0 = __byte_perm(in[0], in[1], 0x5140), t1 = __byte_perm(in[0], in[1], 0x7362);
+    const uint32_t t2 = __byte_perm(in[2], in[3], 0x5140), t3 = __byte_perm(in[2], in[3], 0x7362);
+    out[0] = __byte_perm(t0, t2, 0x5410);
+    out[1] = __byte_perm(t0, t2, 0x7632);
+    out[2] = __byte_perm(t1, t3, 0x5410);
+    out[3] = __byte_perm(t1, t3, 0x7632);
+}
+
+// x as the integer trunc(x 2^(1076 - es)) (es: the largest biased exponent
+// of its row; |result| < 2^54), from the bits of x.
+__device__ __forceinline__ int64_t to_fixed(double x, int es) {
+    const uint32_t h = (uint32_t)__double2hiint(x), l = (uint32_t)__double2loint(x);
+    const int e = (int)((h >> 20) & 0x7FFu);
+    const uint64_t mant = ((uint64_t)((h & 0xFFFFFu) | 0x100000u) << 32) | l;
+    const int sh = es - e - 1;
+    uint64_t mag = sh < 0 ? mant << 1 : (sh < 64 ? mant >> sh : 0);
+    if (e == 0) mag = 0;
+    return (h >> 31) ? -(int64_t)mag : (int64_t)mag;
+}
+
+__global__ void __launch_bounds__(kI8Threads, 1)
+    k_dense_i8(double2 *__restrict__ s, uint64_t nsup, const __grid_constant__ DenseDesc dd,
+               const uint32_t *__restrict__ gW, int *__restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    // full[b]: the digit planes of buffer b written (one arrival per data
+    // warp); accf[r]: the MMAs of accumulator slot r done (tcgen05.commit);
+    // empty[r]: slot r drained (one arrival per data warp); fin: every MMA
+    // the issuer issued has completed
+    __shared__ __align__(8) uint64_t full[2], accf[kI8Slots], empty[kI8Slots], fin;
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int bad_s;
+    // row exponents of supertile it at es_s[it % 3]: a warp writes those of
+    // supertile it + 3 only after every warp has drained supertile it + 1,
+    // i.e. has stored supertile it
+    __shared__ int es_s[3][64];
+    const PassDesc &d = dd.p;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool issuer = warp == kI8DataWarps;
+    if (s_u32(sm) & 1023u) {   // the swizzle pattern needs 1024-byte aligned operands
+        if (tid == 0) atomicExch(err, 2);
+        return;
+    }
+    if (tid == 0) {
+        bad_s = 0;
+        for (int b = 0; b < 2; ++b) mbar_init(&full[b], kI8DataWarps);
+        for (int r = 0; r < kI8Slots; ++r) {
+            mbar_init(&accf[r], 1);
+            mbar_init(&empty[r], kI8DataWarps);
+        }
+        mbar_init(&fin, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (issuer) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_u32(&tmem_slot)),
+                     "r"(kI8TmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    // each CTA takes a contiguous range of supertiles
+    const uint64_t o_lo = nsup * blockIdx.x / gridDim.x, o_hi = nsup * (blockIdx.x + 1) / gridDim.x;
+
+    // data threads.  Split: row n = tid / 8, block indices 8 g .. 8 g + 7, at
+    // lrow + sum of lb[b] over the bits b of the index's low three bits.
+    // Drain: TMEM lane m = 32 q4 + lane (output i' = m / 2, re/im = m & 1),
+    // columns n = 16 cgrp .. + 15; the lane stores n = 16 cgrp + 2 j + (m & 1)
+    // at obase + sum of on[b] over the bits of j.
+    const uint32_t tmask = (1u << d.T) - 1, nmask = tmask & ~dd.blockmask;
+    const int q4 = warp & 3, cgrp = warp >> 2;
+    const uint32_t g = tid & 7, nrow = (uint32_t)tid >> 3;
+    double sw = 0.0;   // W row scale of lane m
+    uint64_t lrow = 0, lb[3] = {0, 0, 0}, obase = 0, on[3] = {0, 0, 0};
+    bool pairs = false;   // block index bit 0 is state bit 0: amplitude pairs are 32-byte runs
+    if (!issuer) {
+        const uint32_t m = 32u * q4 + lane;
+        auto jn = [&](uint32_t v) { return pass_off(deposit_bits(v, nmask), d); };
+        auto jb = [&](uint32_t v) { return pass_off(deposit_bits(v, dd.blockmask), d); };
+        lrow = jn(nrow) + jb(8 * g);
+#pragma unroll
+        for (int b = 0; b < 3; ++b) lb[b] = jb(1u << b);
+        pairs = lb[0] == 1;
+        obase = jb(m >> 1) + jn(16u * cgrp + (m & 1u));
+#pragma unroll
+        for (int b = 0; b < 3; ++b) on[b] = jn(2u << b);
+        // W digit planes into TMEM: lanes 32 q4 .. + 31, columns 56 cgrp .. + 55
+        const uint4 *src = reinterpret_cast<const uint4 *>(gW + (size_t)m * kI8WCols + 56u * cgrp);
+#pragma unroll 1
+        for (int c8 = 0; c8 < 7; ++c8) {
+            const uint4 a = src[2 * c8], b = src[2 * c8 + 1];
+            const uint32_t taddr = tmem + ((32u * q4) << 16) + 56u * cgrp + 8u * c8;
+            asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                         "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                         : "memory");
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        sw = reinterpret_cast<const double *>(gW + 128 * kI8WCols)[m];
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    if (issuer) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool stop = false;
+            for (uint64_t o = o_lo; o < o_hi && !stop && !bad_s; ++o, ++it) {
+                const uint32_t b = it & 1u;
+                if (!tc_wait(&full[b], (it >> 1) & 1u)) {
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t planes = s_u32(sm + b * kI8BufBytes);
+#pragma unroll 1
+                for (int e = 0; e < kI8Weights; ++e) {   // weight wd: products (i, wd - i)
+                    const int wd = kI8LowWeight + e, i0 = max(0, wd - (kI8Digits - 1));
+                    const uint32_t gg = (uint32_t)kI8Weights * it + (uint32_t)e, slot = gg & (kI8Slots - 1);
+                    if (gg >= (uint32_t)kI8Slots && !tc_wait(&empty[slot], ((gg / kI8Slots) - 1) & 1u)) {
+                        stop = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t acc = tmem + kI8AccCol + 64u * slot;
+#pragma unroll 1
+                    for (int i = i0; i <= min(kI8Digits - 1, wd); ++i) {
+                        const int j = wd - i;
+                        const uint32_t idesc = j == kI8Digits - 1 ? kI8IdescS : kI8IdescU;
+                        const uint32_t bplane = planes + (uint32_t)j * kI8PlaneBytes;
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            const uint32_t en = (i != i0 || kk) ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                    acc),
+                                "r"(tmem + 32u * i + 8u * kk), "l"(sw128_desc(bplane + 32u * kk)), "r"(idesc),
+                                "r"(en), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                                : "memory");
+                        }
+                    }
+                    tc_commit(&accf[slot]);
+                }
+            }
+            if (stop) bad_s = 1;
+            // Teardown invariant: the TMEM is released only after every MMA
+            // issued above has completed (one more commit tracks them all).
+            tc_commit(&fin);
+            if (!tc_wait(&fin, 0)) {
+                bad_s = 1;
+                atomicExch(err, 3);
+            }
+        }
+        __syncwarp();
+    } else {
+        // the eight amplitudes of (row nrow, block indices 8 g ..) of supertile o
+        auto load = [&](double2 (&x)[8], uint64_t o) {
+            const double2 *p = s + pass_base(o, d) + lrow;
+            if (pairs) {
+#pragma unroll
+                for (int a = 0; a < 8; a += 2) {
+                    const double *q = reinterpret_cast<const double *>(p + ((a & 2) ? lb[1] : 0) + ((a & 4) ? lb[2] : 0));
+                    double r0, r1, r2, r3;
+                    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                                 : "=d"(r0), "=d"(r1), "=d"(r2), "=d"(r3)
+                                 : "l"(q));
+                    x[a] = make_double2(r0, r1);
+                    x[a + 1] = make_double2(r2, r3);
+                }
+            } else {
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+                    x[a] = p[((a & 1) ? lb[0] : 0) + ((a & 2) ? lb[1] : 0) + ((a & 4) ? lb[2] : 0)];
+            }
+        };
+        // registers -> seven digit planes (row nrow, K chunk g) and the row's exponent
+        auto split = [&](const double2 (&x)[8], unsigned char *planes, int *es_row) {
+            uint32_t ek = 0;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                ek = max(ek, (uint32_t)__double2hiint(x[a].x) & 0x7FF00000u);
+                ek = max(ek, (uint32_t)__double2hiint(x[a].y) & 0x7FF00000u);
+            }
+            ek = max(ek, __shfl_xor_sync(0xffffffffu, ek, 1));
+            ek = max(ek, __shfl_xor_sync(0xffffffffu, ek, 2));
+            ek = max(ek, __shfl_xor_sync(0xffffffffu, ek, 4));
+            const int es = (int)(ek >> 20);
+            if (g == 0) es_row[nrow] = es;
+            uint32_t lo[16], hi[16];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const int64_t vr = to_fixed(x[a].x, es), vi = to_fixed(x[a].y, es);
+                lo[2 * a] = (uint32_t)(uint64_t)vr;
+                hi[2 * a] = (uint32_t)((uint64_t)vr >> 32);
+                lo[2 * a + 1] = (uint32_t)(uint64_t)vi;
+                hi[2 * a + 1] = (uint32_t)((uint64_t)vi >> 32);
+            }
+            uint32_t pl[kI8Digits][4];
+#pragma unroll
+            for (int qd = 0; qd < 4; ++qd) {
+                uint32_t t[4];
+                const uint32_t inl[4] = {lo[4 * qd], lo[4 * qd + 1], lo[4 * qd + 2], lo[4 * qd + 3]};
+                bytes4x4(inl, t);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) pl[j][qd] = t[j];
+                const uint32_t inh[4] = {hi[4 * qd], hi[4 * qd + 1], hi[4 * qd + 2], hi[4 * qd + 3]};
+                bytes4x4(inh, t);
+#pragma unroll
+                for (int j = 4; j < kI8Digits; ++j) pl[j][qd] = t[j - 4];
+            }
+            const uint32_t off = nrow * 128u + ((g ^ (nrow & 7u)) << 4);
+#pragma unroll
+            for (int j = 0; j < kI8Digits; ++j)
+                *reinterpret_cast<uint4 *>(planes + (uint32_t)j * kI8PlaneBytes + off) =
+                    make_uint4(pl[j][0], pl[j][1], pl[j][2], pl[j][3]);
+        };
+        auto wait_warp = [&](uint64_t *bb, uint32_t parity) -> uint32_t {
+            uint32_t dn = 0;
+            if (lane == 0) dn = tc_wait(bb, parity);
+            return __shfl_sync(0xffffffffu, dn, 0);
+        };
+        auto arrive = [&](uint64_t *bb) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bb);
+        };
+        // the seven accumulators of supertile it (at o), combined and stored;
+        // false if a wait ran out
+        auto drain = [&](uint32_t it, uint64_t o) -> bool {
+            double acc[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) acc[c] = 0.0;
+#pragma unroll 1
+            for (int e = 0; e < kI8Weights; ++e) {
+                const uint32_t gg = (uint32_t)kI8Weights * it + (uint32_t)e, slot = gg & (kI8Slots - 1);
+                if (!wait_warp(&accf[slot], (gg / kI8Slots) & 1u)) return false;
+                tc_fence_after();
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((32u * q4) << 16) + kI8AccCol + 64u * slot + 16u * cgrp;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                    "%12, %13, %14, %15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                tc_fence_before();
+                arrive(&empty[slot]);
+                // weight 2^(8 (d - 12)), least significant first.  int32 ->
+                // double exactly on the FP64 pipe: 2^52 + (a + 2^31) has
+                // a + 2^31 as its low mantissa bits
+                const double sc = __hiloint2double((1023 - 96 + 8 * (kI8LowWeight + e)) << 20, 0);
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const double a = __hiloint2double(0x43300000, (int)(r[c] ^ 0x80000000u)) - 4503601774854144.0;
+                    acc[c] = fma(a, sc, acc[c]);
+                }
+            }
+            // scale back and store: lane pairs (re, im) of i' exchange halves
+            const int *es_row = es_s[it % 3];
+            const uint32_t comp = lane & 1u;
+            double2 *out = s + pass_base(o, d) + obase;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e0 = es_row[16 * cgrp + 2 * j], e1 = es_row[16 * cgrp + 2 * j + 1];
+                const double s0 = e0 >= 6 ? __hiloint2double((e0 - 5) << 20, 0) : 0.0;
+                const double s1 = e1 >= 6 ? __hiloint2double((e1 - 5) << 20, 0) : 0.0;
+                const double v0 = acc[2 * j] * sw * s0, v1 = acc[2 * j + 1] * sw * s1;
+                const double keep = comp ? v1 : v0, send = comp ? v0 : v1;
+                const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+                const uint64_t oj = ((j & 1) ? on[0] : 0) + ((j & 2) ? on[1] : 0) + ((j & 4) ? on[2] : 0);
+                out[oj] = comp ? make_double2(recv, keep) : make_double2(keep, recv);
+            }
+            return true;
+        };
+
+        // per supertile: split the registers (supertile o) into plane buffer
+        // it % 2 and hand it to the issuer, load supertile o + 1 into the
+        // registers, then drain and store supertile o - 1 while the MMAs of
+        // o run.  Buffer it % 2 was last read by the MMAs of supertile it - 2,
+        // whose completion this warp saw while draining it.
+        uint32_t it = 0;
+        bool bad = false;
+        double2 x[8];
+        if (o_lo < o_hi) load(x, o_lo);
+        for (uint64_t o = o_lo; o < o_hi; ++o, ++it) {
+            if (__shfl_sync(0xffffffffu, bad_s, 0)) {
+                bad = true;
+                break;
+            }
+            split(x, sm + (it & 1u) * kI8BufBytes, es_s[it % 3]);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            arrive(&full[it & 1u]);
+            if (o + 1 < o_hi) load(x, o + 1);
+            if (it > 0 && !drain(it - 1, o - 1)) {
+                bad = true;
+                break;
+            }
+        }
+        if (!bad && it > 0 && !drain(it - 1, o_hi - 1)) bad = true;
+        if (bad && lane == 0) bad_s = 1;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (bad_s && tid == 0) atomicCAS(err, 0, 1);   // keeps a more specific code (3) set above
+    if (issuer)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kI8TmemCols) : "memory");
+}
+
+// ---- host side ----------------------------------------------------------------
+
+static int biased_exponent(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return (int)((u >> 52) & 0x7FF);
+}
+
+// Digit planes of W = the real embedding of U: row m's entries scaled by
+// 2^(1076 - e_m) (e_m its largest biased exponent), rounded to integers and
+// written as seven balanced base-256 digits; plane i of row m at words
+// m * 224 + 32 i + k / 4 (byte k % 4), then the row scales 2^(e_m - 1028).
+void dense_i8_operand(const DenseBlock &b, std::vector<uint32_t> &out) {
+    out.assign(kI8OperandBytes / 4, 0);
+    unsigned char *bytes = reinterpret_cast<unsigned char *>(out.data());
+    double *scale = reinterpret_cast<double *>(out.data() + kI8OperandWords);
+    for (int m = 0; m < 128; ++m) {
+        const int ip = m >> 1, a = m & 1;
+        double row[128];
+        int em = 0;
+        for (int k = 0; k < 128; ++k) {
+            const int i = k >> 1, c = k & 1;
+            const double ur = b.u[2 * (ip * 64 + i)], ui = b.u[2 * (ip * 64 + i) + 1];
+            row[k] = a == 0 ? (c == 0 ? ur : -ui) : (c == 0 ? ui : ur);
+            em = std::max(em, biased_exponent(row[k]));
+        }
+        scale[m] = em > 0 ? std::ldexp(1.0, em - 1028) : 0.0;
+        if (em == 0) continue;
+        for (int k = 0; k < 128; ++k) {
+            long long v = std::llrint(std::ldexp(row[k], 1076 - em));
+            for (int i = 0; i < kI8Digits; ++i) {
+                int dg;
+                if (i < kI8Digits - 1) {
+                    dg = (int)((v + 128) & 255) - 128;
+                    v = (v - dg) / 256;
+                } else {
+                    dg = (int)v;   // |v| <= 65 after six balanced digits of a 55-bit value
+                }
+                bytes[((size_t)m * kI8WCols + 32u * i + (unsigned)k / 4) * 4 + (unsigned)k % 4] = (unsigned char)(int8_t)dg;
+            }
+        }
+    }
+}
+
+int launch_dense_i8(double2 *state, int n, const DenseDesc &dd, const uint32_t *dW, int *derr, cudaStream_t st) {
+    if (n < kI8TileBits || dd.p.T != kI8TileBits || dd.p.L < 1 || __builtin_popcount(dd.blockmask) != kDenseQubits)
+        return fail(QK_ERR_ARG, "complex128 tensor-core blocks need >= %d qubits", kI8TileBits);
+    static std::atomic<uint64_t> smem_done{0};
+    const cudaError_t ea = smem_limit_once(smem_done, (const void *)k_dense_i8, (int)kI8Smem);
+    if (ea != cudaSuccess) return fail(QK_ERR_CUDA, "cudaFuncSetAttribute(k_dense_i8): %s", cudaGetErrorString(ea));
+    const uint64_t nsup = 1ull << (n - kI8TileBits);
+    const unsigned grid = (unsigned)std::min<uint64_t>(nsup, (uint64_t)device_sms());
+    k_dense_i8<<<grid, kI8Threads, kI8Smem, st>>>(state, nsup, dd, dW, derr);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : fail(QK_ERR_CUDA, "k_dense_i8 launch: %s", cudaGetErrorString(e));
+}
+
+}  // namespace qk

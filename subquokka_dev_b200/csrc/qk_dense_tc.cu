@@ -41,6 +41,7 @@
 #include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_pass_device.cuh"
+#include "qk_tc_device.cuh"
 
 namespace qk {
 
@@ -51,12 +52,6 @@ constexpr int kTcMinTileBits = 12;                    // 64 x 64
 constexpr uint32_t kTcOpBytes = 128 * 128 * 2;        // one 128 x 128 bf16 operand
 constexpr uint32_t kTcSmem = 6 * kTcOpBytes;          // W hi/lo + two state buffers hi/lo
 constexpr uint32_t kTcTmemCols = 256;                 // two 128-column accumulators
-constexpr long long kTcWaitLimit = 20000000;          // mbarrier polls before giving up
-
-struct DenseDesc {
-    PassDesc p;         // tile bits (T = 13, or 12), L
-    uint32_t blockmask; // tile-local bits that are the block's qubits
-};
 
 // Byte offset of element (row r, k) of a 128-row x 128-K bf16 operand in the
 // canonical K-major 128-byte-swizzle layout: two K atoms of 64 elements (16 KB
@@ -66,25 +61,14 @@ __host__ __device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t k) {
     return (k >> 6) * 16384u + r * 128u + ((((k >> 3) & 7u) ^ (r & 7u)) << 4) + (k & 7u) * 2u;
 }
 
-__device__ __forceinline__ uint32_t s_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 // Shared-memory descriptor of MMA step kk (K = 16 kk .. 16 kk + 15) of an
 // operand at saddr (1024-byte aligned): the step's 32 bytes inside its atom.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, int kk) {
-    const uint32_t a = saddr + (uint32_t)(kk >> 2) * 16384u + (uint32_t)(kk & 3) * 32u;
-    uint64_t d = (uint64_t)((a >> 4) & 0x3FFFu);
-    d |= (uint64_t)1 << 16;                          // leading byte offset: unused (swizzled K-major)
-    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;   // stride byte offset: next 8-row group
-    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
-    d |= (uint64_t)2 << 61;                          // 128-byte swizzle
-    return d;
+    return sw128_desc(saddr + (uint32_t)(kk >> 2) * 16384u + (uint32_t)(kk & 3) * 32u);
 }
 
 // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 __device__ __forceinline__ void store_bf16x8(unsigned char *dst, const float *v) {
     uint4 w;
@@ -95,20 +79,6 @@ __device__ __forceinline__ void store_bf16x8(unsigned char *dst, const float *v)
         u[k] = *reinterpret_cast<const uint32_t *>(&h);
     }
     *reinterpret_cast<uint4 *>(dst) = w;
-}
-
-// Bounded wait for the phase with parity `parity` of bar.
-__device__ __forceinline__ uint32_t tc_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t done = 0;
-    for (long long t = 0; t < kTcWaitLimit && !done; ++t) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(s_u32(bar)), "r"(parity)
-            : "memory");
-    }
-    return done;
 }
 
 // Per-thread work of one supertile, two layouts:
@@ -483,13 +453,13 @@ void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out) {
 }
 
 // tile bits of a block: its six qubits plus the lowest other state bits, up
-// to 13 (64 x 128 supertiles)
-DenseDesc dense_block_desc(const DenseBlock &b, int n) {
+// to max_tile_bits (13: 64 x 128 supertiles)
+DenseDesc dense_block_desc(const DenseBlock &b, int n, int max_tile_bits) {
     DenseDesc dd;
     std::memset(&dd, 0, sizeof dd);
     std::vector<char> in(n, 0);
     for (int k = 0; k < kDenseQubits; ++k) in[b.q[k]] = 1;
-    const int tbits = std::min(n, kTcMaxTileBits);
+    const int tbits = std::min(n, max_tile_bits);
     int cnt = kDenseQubits;
     for (int q = 0; q < n && cnt < tbits; ++q)
         if (!in[q]) { in[q] = 1; ++cnt; }
@@ -534,12 +504,25 @@ int launch_dense_tc(float2 *state, int n, const DenseDesc &dd, const uint16_t *d
 // from qk_pass.cu: one VSWAP as a permutation pass
 int apply_perm_gate(void *state, int n, int dtype, const Op &op, cudaStream_t st);
 
-int run_dense_blocks(void *state, int n, const std::vector<DenseBlock> &blocks, const uint16_t *dA, int *derr,
+int launch_dense_i8(double2 *state, int n, const DenseDesc &dd, const uint32_t *dW, int *derr, cudaStream_t st);
+
+size_t dense_operand_bytes(int dtype) { return dtype == QK_C128 ? kI8OperandBytes : 2 * (size_t)kTcOpBytes; }
+
+int run_dense_blocks(void *state, int n, int dtype, const std::vector<DenseBlock> &blocks, const void *dA, int *derr,
                      cudaStream_t st) {
+    const unsigned char *ops = static_cast<const unsigned char *>(dA);
+    const size_t step = dense_operand_bytes(dtype);
     for (size_t k = 0; k < blocks.size(); ++k) {
         const DenseBlock &b = blocks[k];
-        int rc = b.perm ? apply_perm_gate(state, n, QK_C64, b.perm_op, st)
-                        : launch_dense_tc((float2 *)state, n, dense_block_desc(b, n), dA + k * 2 * 128 * 128, derr, st);
+        int rc;
+        if (b.perm)
+            rc = apply_perm_gate(state, n, dtype, b.perm_op, st);
+        else if (dtype == QK_C128)
+            rc = launch_dense_i8((double2 *)state, n, dense_block_desc(b, n, kI8TileBits),
+                                 reinterpret_cast<const uint32_t *>(ops + k * step), derr, st);
+        else
+            rc = launch_dense_tc((float2 *)state, n, dense_block_desc(b, n, kTcMaxTileBits),
+                                 reinterpret_cast<const uint16_t *>(ops + k * step), derr, st);
         if (rc) return rc;
     }
     return QK_OK;

@@ -167,8 +167,27 @@ struct DenseBlock {
     int ngates = 0;
 };
 // width (5 or 6): most qubits a block's gates may touch; blocks are padded to
-// kDenseQubits with idle qubits.
-int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::vector<DenseBlock> &blocks);
+// kDenseQubits with idle qubits.  dtype sets the tile limits of the
+// permutation blocks.
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, int dtype, std::vector<DenseBlock> &blocks);
+
+// A dense block's pass over the state: a supertile is the block's qubits plus
+// the lowest other state bits (tile-local bits ascending in state position).
+struct DenseDesc {
+    PassDesc p;         // tile bits T, contiguous run L
+    uint32_t blockmask; // tile-local bits that are the block's qubits
+};
+DenseDesc dense_block_desc(const DenseBlock &b, int n, int max_tile_bits);
+
+// complex128 blocks (qk_dense_i8.cu): 64 x 64 supertiles; the operand of a
+// block is its digit planes (128 rows x 224 words) and 128 row scales.
+constexpr int kI8TileBits = 12;
+constexpr int kI8Digits = 7;
+constexpr size_t kI8OperandWords = 128 * 32 * kI8Digits;
+constexpr size_t kI8OperandBytes = kI8OperandWords * 4 + 128 * sizeof(double);
+void dense_i8_operand(const DenseBlock &b, std::vector<uint32_t> &out);   // kI8OperandBytes / 4 words
+// Bytes of one block's device operand for dtype.
+size_t dense_operand_bytes(int dtype);
 // Backward sweep of an adjoint gradient: the inverses of gates[ng-1..0] on
 // (psi, lambda), with the gradient of trainable gates (pidx[i] >= 0) taken
 // just before their inverse.

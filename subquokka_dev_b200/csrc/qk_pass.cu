@@ -326,9 +326,9 @@ int run_plan_at(void *state, int dtype, const HostPlan &hp, const TOp *ops, cons
 using namespace qk;
 
 namespace qk {
-struct DenseDesc;
 void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out);
-int run_dense_blocks(void *state, int n, const std::vector<DenseBlock> &blocks, const uint16_t *dA, int *derr,
+// the blocks of a dense plan in order (qk_dense_tc.cu)
+int run_dense_blocks(void *state, int n, int dtype, const std::vector<DenseBlock> &blocks, const void *dA, int *derr,
                      cudaStream_t st);
 }  // namespace qk
 
@@ -336,10 +336,10 @@ struct qk_plan {
     HostPlan hp;
     DevPlan dp;
     bool uploaded = false;
-    // fuse_width = 6: dense blocks on the tensor cores instead of passes
+    // fuse_width = 5 or 6: dense blocks on the tensor cores instead of passes
     bool dense = false;
     std::vector<DenseBlock> blocks;
-    uint16_t *dA = nullptr;
+    void *dA = nullptr;
     int *derr = nullptr;
 };
 
@@ -382,13 +382,13 @@ int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_op
     if (opts && opts->fuse_width) {
         if (opts->fuse_width != 5 && opts->fuse_width != kDenseQubits)
             return fail(QK_ERR_ARG, "fuse_width must be 0, 5 or %d", kDenseQubits);
-        if (dtype != QK_C64) return fail(QK_ERR_UNSUPPORTED, "tensor-core dense blocks run on complex64 states");
+        if (dtype != QK_C64 && dtype != QK_C128) return fail(QK_ERR_ARG, "unknown dtype %d", dtype);
         if (nqubits < 12) return fail(QK_ERR_UNSUPPORTED, "tensor-core dense blocks need at least 12 qubits");
         auto *p = new qk_plan();
         p->dense = true;
         p->hp.n = nqubits;
         p->hp.dtype = dtype;
-        int rc = build_dense_blocks(gates, n, nqubits, opts->fuse_width, p->blocks);
+        int rc = build_dense_blocks(gates, n, nqubits, opts->fuse_width, dtype, p->blocks);
         if (rc) {
             delete p;
             return rc;
@@ -460,16 +460,25 @@ namespace qk {
 int plan_prepare(qk_sv *sv, qk_plan *p) {
     if (p->uploaded) return QK_OK;
     if (p->dense) {
-        std::vector<uint16_t> all, one;
-        for (const auto &b : p->blocks) {
-            if (b.perm) one.assign(2 * 128 * 128, 0);
-            else dense_block_operand(b, one);
-            all.insert(all.end(), one.begin(), one.end());
+        // one operand per block (zeros for permutation blocks), dense_operand_bytes apart
+        const size_t step = dense_operand_bytes(p->hp.dtype);
+        std::vector<unsigned char> all(p->blocks.size() * step, 0);
+        std::vector<uint16_t> one16;
+        std::vector<uint32_t> one32;
+        for (size_t k = 0; k < p->blocks.size(); ++k) {
+            const DenseBlock &b = p->blocks[k];
+            if (b.perm) continue;
+            if (p->hp.dtype == QK_C128) {
+                dense_i8_operand(b, one32);
+                std::memcpy(all.data() + k * step, one32.data(), step);
+            } else {
+                dense_block_operand(b, one16);
+                std::memcpy(all.data() + k * step, one16.data(), step);
+            }
         }
-        cudaError_t e = cudaMalloc(&p->dA, std::max<size_t>(1, all.size()) * sizeof(uint16_t));
+        cudaError_t e = cudaMalloc(&p->dA, std::max<size_t>(1, all.size()));
         if (e == cudaSuccess) e = cudaMalloc(&p->derr, sizeof(int));
-        if (e == cudaSuccess && !all.empty())
-            e = cudaMemcpy(p->dA, all.data(), all.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !all.empty()) e = cudaMemcpy(p->dA, all.data(), all.size(), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return cuda_err(e, "upload dense blocks");
     } else {
         int rc = upload_plan(p->hp, p->hp.dtype, p->dp, state_stream(sv));
@@ -495,7 +504,7 @@ int qk_plan_apply(qk_sv *sv, qk_plan *p) {
         cudaStream_t st = state_stream(sv);
         cudaError_t e = cudaMemsetAsync(p->derr, 0, sizeof(int), st);
         if (e != cudaSuccess) return cuda_err(e, "reset error flag");
-        rc = run_dense_blocks(state_ptr(sv), p->hp.n, p->blocks, p->dA, p->derr, st);
+        rc = run_dense_blocks(state_ptr(sv), p->hp.n, p->hp.dtype, p->blocks, p->dA, p->derr, st);
         if (rc) return rc;
         int herr = 0;
         e = cudaMemcpyAsync(&herr, p->derr, sizeof(int), cudaMemcpyDeviceToHost, st);

@@ -34,10 +34,13 @@ namespace qk {
 PlanOptions default_plan_options(int dtype, int n) {
     PlanOptions o;
     o.dtype = dtype;
-    // complex128: 2048-amplitude tiles, 16 amplitudes a thread (128 threads,
-    // 241 registers): 0.75 s on the 30-qubit random circuit against 0.87 s
-    // for (12, 3), the per-op program overhead spread over more FP64 work
-    o.tile_bits = std::min(n, dtype == QK_C128 ? 11 : 13);
+    // 2048-amplitude tiles, 16 amplitudes a thread (128 threads).  complex128:
+    // 0.75 s on the 30-qubit random circuit against 0.87 s for (12, 3), the
+    // per-op program overhead spread over more FP64 work.  complex64: more
+    // passes than with 8192-amplitude tiles (31 against 21 on that circuit)
+    // but shorter ones: 355 against 389 ms there, 3.73 against 3.99 s on the
+    // 33-qubit 24-layer circuit, 181 against 185 ms on the 30-qubit QFT
+    o.tile_bits = std::min(n, 11);
     o.reg_bits = std::min(o.tile_bits, 4);
     return o;
 }
@@ -833,7 +836,7 @@ static void dense_partition(const std::vector<Op> &ops, int n, int width, int ns
     }
 }
 
-int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::vector<DenseBlock> &blocks) {
+int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, int dtype, std::vector<DenseBlock> &blocks) {
     if (n < kDenseQubits) return fail(QK_ERR_ARG, "dense blocks need at least %d qubits", kDenseQubits);
     if (width < 2 || width > kDenseQubits) return fail(QK_ERR_ARG, "block width must be in [2, %d], got %d", kDenseQubits, width);
     std::vector<Op> ops;
@@ -841,7 +844,7 @@ int build_dense_blocks(const qk_gate *gates, size_t ng, int n, int width, std::v
     if (rc) return rc;
     // at most three pairs per restoring permutation: a permutation block
     // lists its targets in kDenseQubits entries
-    relabel_perms(ops, n, low_bits(QK_C64), perm_tile_bits(QK_C64), kDenseQubits / 2, false);
+    relabel_perms(ops, n, low_bits(dtype), perm_tile_bits(dtype), kDenseQubits / 2, false);
     // The fuser is greedy, and which greedy choice needs the fewest blocks
     // depends on the circuit: the list as given and its ASAP layering, each
     // with 1, 4 and 16 seed ops per block, are partitioned (block counts

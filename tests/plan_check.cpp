@@ -237,9 +237,11 @@ int main() {
         }
         // tensor-core dense blocks (64 x 64 unitaries on six qubits, block
         // index bit b = qubit q[b]; permutation blocks for the restore)
-        for (int width : {5, 6}) {
+        // (both dtypes: their permutation blocks have different tile limits)
+        for (int form = 0; form < 4; ++form) {
+            const int width = 5 + (form & 1), dtype = form < 2 ? QK_C64 : QK_C128;
             std::vector<qk::DenseBlock> blocks;
-            if (qk::build_dense_blocks(gates.data(), gates.size(), n, width, blocks)) {
+            if (qk::build_dense_blocks(gates.data(), gates.size(), n, width, dtype, blocks)) {
                 std::printf("seed %d: build_dense_blocks failed: %s\n", seed, qk_last_error());
                 ++bad;
                 continue;
@@ -265,7 +267,8 @@ int main() {
             }
             const double dd = max_diff(want, have);
             if (dd > 1e-12) {
-                std::printf("dense seed %d width %d: max |d amp| %.3g, %zu blocks\n", seed, width, dd, blocks.size());
+                std::printf("dense seed %d width %d dtype %d: max |d amp| %.3g, %zu blocks\n", seed, width, dtype, dd,
+                            blocks.size());
                 ++bad;
             }
         }

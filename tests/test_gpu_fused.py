@@ -184,3 +184,68 @@ def test_tensor_core_block_sequences(n, blocks):
     out = run_plan(n, circ, init, "c64", fuse_width=6)
     assert fidelity_err(out, ref) <= 1e-6
     assert np.abs(out - ref).max() <= 5e-5
+
+
+# complex128 dense blocks: the same blocks as exact integer contractions on the
+# int8 tensor cores (seven 8-bit digits an operand row, 28 digit products,
+# int32 accumulate, FP64 recombination): within 1e-12 of the FP64 oracle
+TOL_C128_TC = 1e-12
+
+
+@pytest.mark.parametrize("n,width", [(12, 6), (13, 6), (14, 6), (17, 6), (13, 5), (18, 5)])
+def test_tensor_core_c128_dense_blocks(n, width):
+    circ = random_circuit(n, 200, 500 + n)
+    init = circuits.random_state(n, 41)
+    ref = oracle.apply_circuit(init, n, circ)
+    out = run_plan(n, circ, init, "c128", fuse_width=width)
+    assert np.abs(out - ref).max() <= TOL_C128_TC
+    assert fidelity_err(out, ref) <= 1e-15   # the FP64 rounding floor of fidelity_err
+
+
+def test_tensor_core_c128_random_circuit_family():
+    # from |0>: early blocks see rows of zeros
+    n = 20
+    circ = circuits.random_u3_cz(n, 8, 40)
+    ref = oracle.apply_circuit(zero(n), n, circ)
+    out = run_plan(n, circ, None, "c128", fuse_width=6)
+    assert np.abs(out - ref).max() <= TOL_C128_TC
+
+
+@pytest.mark.parametrize("n,blocks", [
+    (16, [[0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11]]),
+    (16, [[6, 7, 8, 9, 10, 11], [0, 1, 2, 3, 4, 5]]),
+    (16, [[0, 1, 2, 8, 9, 10], [0, 3, 4, 5, 12, 13]]),
+    (16, [[3, 4, 5, 6, 7, 8], [9, 10, 11, 12, 13, 14]]),
+    (16, [[2, 5, 7, 9, 11, 13], [1, 4, 6, 8, 10, 15]]),
+    (12, [[0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11]]),          # one supertile
+    (15, [[0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11], [3, 4, 5, 12, 13, 14]]),
+])
+def test_tensor_core_c128_block_sequences(n, blocks):
+    circ = block_circuit(blocks, 9 + n)
+    p = Plan(circ, n, "c128", fuse_width=6)
+    got = [p.dense_block(k)[0] for k in range(p.stats()[0])]
+    assert len(got) == len(blocks) and got[:2] == blocks[:2]
+    p.close()
+    init = circuits.random_state(n, 10)
+    ref = oracle.apply_circuit(init, n, circ)
+    out = run_plan(n, circ, init, "c128", fuse_width=6)
+    assert np.abs(out - ref).max() <= TOL_C128_TC
+
+
+def test_tensor_core_c128_wide_dynamic_range():
+    # amplitudes spread over 2^-200 .. 1 and exact zeros: each row of a
+    # supertile is scaled by its own largest entry, so small rows keep their
+    # relative precision
+    n = 14
+    rng = np.random.default_rng(12)
+    init = circuits.random_state(n, 13) * np.exp2(-rng.integers(0, 200, 1 << n))
+    init[rng.random(1 << n) < 0.1] = 0
+    circ = block_circuit([[1, 3, 5, 7, 9, 11], [0, 2, 4, 6, 8, 10]], 14)
+    ref = oracle.apply_circuit(init, n, circ)
+    out = run_plan(n, circ, init, "c128", fuse_width=6)
+    assert np.abs(out - ref).max() <= 1e-15
+    # the whole state scaled by 2^-900: the same relative error
+    tiny = circuits.random_state(n, 15) * np.exp2(-900)
+    ref = oracle.apply_circuit(tiny, n, circ)
+    out = run_plan(n, circ, tiny, "c128", fuse_width=6)
+    assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()

@@ -159,5 +159,7 @@ def test_dense_fuser_block_count():
     c = circuits.random_u3_cz(33, 24, 33)
     nb = Plan(c, 33, "c64", fuse_width=6).stats()[0]
     assert nb < c.ngates / 4
+    # complex128 blocks (int8 tensor cores) use the same fuser
+    assert Plan(c, 33, "c128", fuse_width=6).stats()[0] == nb
     with pytest.raises(sq.QkError):
-        Plan(c, 33, "c128", fuse_width=6)
+        Plan(circuits.random_u3_cz(11, 2, 3), 11, "c128", fuse_width=6)
