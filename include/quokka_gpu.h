@@ -247,16 +247,20 @@ int qk_apply_gates_timed(qk_sv *sv, const qk_gate *gates, size_t n, float *gate_
 /* Options of a fused plan; zero fields take the defaults. */
 typedef struct qk_plan_opts {
     int32_t dtype;        /* qk_dtype of the states the plan runs on        */
-    int32_t tile_bits;    /* qubits per shared-memory tile (default 12 for
-                             complex128, 13 for complex64; at most 14)      */
-    int32_t reg_bits;     /* qubits held in registers per thread (default 3
-                             for complex128, 4 for complex64; at most 5)    */
+    int32_t tile_bits;    /* qubits per shared-memory tile (default 11; at
+                             most 14)                                       */
+    int32_t reg_bits;     /* qubits held in registers per thread (default 4;
+                             at most 5)                                     */
     int32_t fuse_width;   /* 0: register passes.  5 or 6: gates fused into
                              dense unitaries on at most that many qubits
                              (FP64 on the host, padded to 6 qubits), each
                              applied as a 64 x 64 complex contraction on the
-                             tensor cores in split precision (3 x BF16, FP32
-                             accumulate); complex64 states of >= 12 qubits */
+                             tensor cores, for states of >= 12 qubits:
+                             complex64 in split precision (3 x BF16, FP32
+                             accumulate); complex128 exactly in integer
+                             arithmetic (seven 8-bit digits an operand row,
+                             int8 products, int32 accumulate, FP64
+                             recombination), within about 2^-48 of FP64 */
     int32_t reserved[4];
 } qk_plan_opts;
 
@@ -274,8 +278,8 @@ typedef struct qk_plan qk_plan;
 int qk_plan_create(const qk_gate *gates, size_t n, int nqubits, const qk_plan_opts *opts, qk_plan **out);
 /* The plan of a subcircuit file that qk_apply_groups runs: the gates of all
  * groups fused as one list, VSWAPs as renamings of the qubits after them.
- * With opts->fuse_width 5 or 6 (complex64): tensor-core dense blocks over
- * the same list, as qk_plan_create makes them. */
+ * With opts->fuse_width 5 or 6: tensor-core dense blocks over the same list,
+ * as qk_plan_create makes them. */
 int qk_plan_create_groups(const qk_gate *gates, const int32_t *group_sizes, size_t ngroups, int nqubits,
                           const qk_plan_opts *opts, qk_plan **out);
 /* Number of passes, program operations and register re-mappings. */

@@ -13,44 +13,38 @@
 // kind::i8, int32 accumulators), an Ozaki-type split:
 //
 //   - every row of W and every row n of S is scaled by a power of two to a
-//     55-bit integer v (|v| < 2^54): W rows on the host, rounded, as seven
-//     balanced digits in [-128, 127]; state rows on the device, truncated,
-//     as the seven low bytes of v in two's complement (six unsigned digits
-//     and a signed top digit in [-64, 63]);
+//     55-bit integer v = round(x 2^(1076 - e)) (e = the row's largest biased
+//     exponent, |v| < 2^54) and cut into seven 8-bit digits: W rows on the
+//     host as balanced digits in [-128, 127]; state rows on the device as
+//     the seven low bytes of v in two's complement (six unsigned digits and
+//     a signed top digit in [-64, 63]);
 //   - sum_k v_w v_s = sum_(i, j) 2^(8 (i + j)) sum_k w_i s_j.  The 28 digit
 //     products with i + j >= 6 are computed; the dropped ones lie below
-//     2^-50 of the result.  Products of one weight d = i + j add up in one
-//     int32 accumulator (|sum| <= 7 x 128 x 128 x 255 < 2^25);
+//     2^-48 of the largest result of the row.  Products of one weight
+//     d = i + j add up in one int32 accumulator (|sum| <= 7 x 128 x 128 x 255
+//     < 2^25);
 //   - the seven accumulators of a supertile are combined in FP64 and scaled
-//     back (2^(e_w - 1028) 2^(e_s - 1028), e = the row's largest biased
-//     exponent).  Rows whose largest entry is below 2^-1017 come out as zero.
-//
-// The result matches FP64 arithmetic to about 2^-50 relative per block.
+//     back by 2^(e_w - 1028) 2^(e_s - 1028).  Rows whose largest entry is
+//     below 2^-1017 come out as zero.
 //
 // Operands and memory:
-//   - W's digit planes are the A operand in tensor memory (lane m = row m,
-//     four digits of consecutive k per 32-bit column; plane i at columns
-//     32 i .. 32 i + 31), loaded once per CTA with tcgen05.st.
+//   - W's digit planes are the A operand in shared memory (M = 128 rows m,
+//     K-major, 128-byte swizzle: 16 KiB a plane), copied once per CTA.
 //   - The state's digit planes are the B operand in shared memory (N = 64
-//     rows n, K-major, 128-byte swizzle: 8 KiB a plane, seven planes).
-//   - Accumulators D[m][n]: four slots of 64 columns (a ring over the seven
-//     weights of consecutive supertiles), TMEM columns 256 .. 511.
-//   - Raw supertiles (64 KiB of complex128) are staged in shared memory by
-//     cp.async, two buffers, so that the load of supertile s + 2 runs while
-//     s and s + 1 are processed; their 16-byte slots are XOR-swizzled so that
-//     both the coalesced copy and the per-row reads are free of bank
-//     conflicts.
+//     rows n, 8 KiB a plane), two supertiles' worth.
+//   - Accumulators D[m][n]: eight slots of 64 TMEM columns, a ring over the
+//     seven weights of consecutive supertiles, so that the MMAs of a whole
+//     supertile can be issued while the one before is drained.
 //
 // Roles (16 data warps + 1 issuer warp): per supertile the data warps split
-// the staged amplitudes into digit planes (thread = row n, block indices
-// 8 g .. 8 g + 7), hand them to the issuer, refill the staging buffer, then
-// drain the seven accumulators as their MMAs complete (thread = TMEM lane m,
-// 16 columns n), combine them in FP64 and store the supertile.  One elected
-// thread issues the 28 x 4 MMAs (M128 N64 K32) of a supertile and commits
-// each weight's accumulator to an mbarrier.  Every wait is bounded: a wait
-// that runs out sets an error code (1), the data warps agree on stopping at
-// their next barrier, and the issuer releases the TMEM only after its last
-// MMAs have completed (3 if that wait runs out).
+// the amplitudes they loaded into digit planes (thread = row n, block
+// indices 8 g .. 8 g + 7), hand them to the issuer, load the next supertile,
+// then drain the seven accumulators of the previous one (thread = TMEM lane
+// m, 16 columns n), combine them in FP64 and store it.  One elected thread
+// issues the 28 x 4 MMAs (M128 N64 K32) of a supertile and commits each
+// weight's accumulator to an mbarrier.  Every wait is bounded: a wait that
+// runs out sets an error code (1) and the warp stops; the issuer releases the
+// TMEM only after its last MMAs have completed (3 if that wait runs out).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -68,16 +62,17 @@ namespace qk {
 constexpr int kI8DataWarps = 16;
 constexpr int kI8DataThreads = 32 * kI8DataWarps;
 constexpr int kI8Threads = kI8DataThreads + 32;             // + one MMA-issuer warp
+constexpr uint32_t kI8WPlaneBytes = 128u * 128u;            // one digit plane of W
 constexpr uint32_t kI8PlaneBytes = 64u * 128u;              // one digit plane of the state operand
+constexpr uint32_t kI8WBytes = kI8Digits * kI8WPlaneBytes;  // 112 KiB
 constexpr uint32_t kI8BufBytes = kI8Digits * kI8PlaneBytes; // the seven planes of one supertile
-constexpr uint32_t kI8Smem = 2u * kI8BufBytes;              // two supertiles: 112 KiB
-constexpr uint32_t kI8WCols = 32u * kI8Digits;              // W digit planes, TMEM columns 0 .. 223
-constexpr uint32_t kI8AccCol = 256;                         // accumulator slot r at 256 + 64 r
-constexpr int kI8Slots = 4;
+constexpr uint32_t kI8Smem = kI8WBytes + 2u * kI8BufBytes;  // 224 KiB
+constexpr int kI8Slots = 8;                                 // accumulators of 64 columns
 constexpr int kI8LowWeight = 6;                             // digit products of weight i + j >= this
 constexpr int kI8Weights = 2 * (kI8Digits - 1) + 1 - kI8LowWeight;
-constexpr uint32_t kI8TmemCols = 512;
-static_assert(kI8WCols <= kI8AccCol, "digit planes overlap the accumulators");
+constexpr uint32_t kI8TmemCols = 64u * kI8Slots;
+static_assert(kI8TmemCols <= 512, "accumulators exceed the tensor memory");
+static_assert(kI8WBytes == kI8OperandWords * 4, "operand layout");
 
 // kind::i8, D = S32, A = W digits (signed), B = state digits (unsigned for
 // planes 0-5, signed for the top plane), both K-major, M = 128, N = 64
@@ -94,16 +89,20 @@ __device__ __forceinline__ void bytes4x4(const uint32_t (&in)[4], uint32_t (&out
     out[3] = __byte_perm(t1, t3, 0x7632);
 }
 
-// x as the integer trunc(x 2^(1076 - es)) (es: the largest biased exponent
-// of its row; |result| < 2^54), from the bits of x.
-__device__ __forceinline__ int64_t to_fixed(double x, int es) {
-    const uint32_t h = (uint32_t)__double2hiint(x), l = (uint32_t)__double2loint(x);
-    const int e = (int)((h >> 20) & 0x7FFu);
-    const uint64_t mant = ((uint64_t)((h & 0xFFFFFu) | 0x100000u) << 32) | l;
-    const int sh = es - e - 1;
-    uint64_t mag = sh < 0 ? mant << 1 : (sh < 64 ? mant >> sh : 0);
-    if (e == 0) mag = 0;
-    return (h >> 31) ? -(int64_t)mag : (int64_t)mag;
+// round(x 2^(1076 - es)) as two's-complement words (lo, hi), es being the
+// largest biased exponent of x's row, with `scale` = 2^(1044 - es): y = x
+// scale (|y| < 2^22) splits exactly into rint(y) and r = y - rint(y)
+// (|r| <= 1/2), and rint(y) 2^32 + rint(r 2^32) = round(x 2^(1076 - es)).
+// Each integer is read off the low mantissa bits of 1.5 2^52 + value; bits
+// 32.. of the second one's mantissa say whether rint(r 2^32) was negative.
+__device__ __forceinline__ void to_fixed(double x, double scale, uint32_t &lo, uint32_t &hi) {
+    const double magic = 6755399441055744.0;   // 1.5 2^52
+    const double t1 = fma(x, scale, magic);
+    const double yh = t1 - magic;
+    const double r = fma(x, scale, -yh);
+    const double t2 = fma(r, 4294967296.0, magic);
+    lo = (uint32_t)__double2loint(t2);
+    hi = (uint32_t)__double2loint(t1) + ((uint32_t)__double2hiint(t2) & 0xFFFFFu) - 0x80000u;
 }
 
 __global__ void __launch_bounds__(kI8Threads, 1)
@@ -117,11 +116,12 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     __shared__ __align__(8) uint64_t full[2], accf[kI8Slots], empty[kI8Slots], fin;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int bad_s;
-    // row exponents of supertile it at es_s[it % 3]: a warp writes those of
-    // supertile it + 3 only after every warp has drained supertile it + 1,
-    // i.e. has stored supertile it
-    __shared__ int es_s[3][64];
+    // column scales 2^(e_s - 1028) of supertile it at ss_s[it % 3]: a warp
+    // writes those of supertile it + 3 only after every warp has drained the
+    // last weight of supertile it + 1, i.e. has stored supertile it
+    __shared__ __align__(16) double ss_s[3][64];
     const PassDesc &d = dd.p;
+    unsigned char *sW = sm, *sB = sm + kI8WBytes;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool issuer = warp == kI8DataWarps;
     if (s_u32(sm) & 1023u) {   // the swizzle pattern needs 1024-byte aligned operands
@@ -144,6 +144,37 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // W's digit planes (already in the swizzled operand layout) into shared memory
+    for (uint32_t i = tid; i < kI8WBytes / 16; i += kI8Threads)
+        reinterpret_cast<uint4 *>(sW)[i] = reinterpret_cast<const uint4 *>(gW)[i];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+
+    // data threads.  Split: row n = tid / 8, block indices 8 g .. 8 g + 7, at
+    // lrow + sum of 2^lbp[b] over the bits b of the index's low three bits.
+    // Drain: TMEM lane m = 32 q4 + lane (output i' = m / 2, re/im = m & 1),
+    // columns n = 16 cgrp .. + 15; the lane stores n = 16 cgrp + 2 j + (m & 1)
+    // at obase + sum of 2^onp[b] over the bits of j.  (lbp, onp: the state
+    // bits of single tile bits, packed a byte each.)
+    const uint32_t tmask = (1u << d.T) - 1, nmask = tmask & ~dd.blockmask;
+    const int q4 = warp & 3, cgrp = warp >> 2;
+    const uint32_t g = tid & 7, nrow = (uint32_t)tid >> 3;
+    double sw = 0.0;   // W row scale of lane m
+    uint64_t lrow = 0, obase = 0;
+    uint32_t lbp = 0, onp = 0;
+    auto bitoff = [](uint32_t packed, int b) { return 1ull << ((packed >> (8 * b)) & 63u); };
+    if (!issuer) {
+        const uint32_t m = 32u * q4 + lane;
+        auto jn = [&](uint32_t v) { return pass_off(deposit_bits(v, nmask), d); };
+        auto jb = [&](uint32_t v) { return pass_off(deposit_bits(v, dd.blockmask), d); };
+        lrow = jn(nrow) + jb(8 * g);
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            lbp |= (uint32_t)(__ffsll((long long)jb(1u << b)) - 1) << (8 * b);
+            onp |= (uint32_t)(__ffsll((long long)jn(2u << b)) - 1) << (8 * b);
+        }
+        obase = jb(m >> 1) + jn(16u * cgrp + (m & 1u));
+        sw = reinterpret_cast<const double *>(gW + kI8OperandWords)[m];
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -151,49 +182,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     // each CTA takes a contiguous range of supertiles
     const uint64_t o_lo = nsup * blockIdx.x / gridDim.x, o_hi = nsup * (blockIdx.x + 1) / gridDim.x;
 
-    // data threads.  Split: row n = tid / 8, block indices 8 g .. 8 g + 7, at
-    // lrow + sum of lb[b] over the bits b of the index's low three bits.
-    // Drain: TMEM lane m = 32 q4 + lane (output i' = m / 2, re/im = m & 1),
-    // columns n = 16 cgrp .. + 15; the lane stores n = 16 cgrp + 2 j + (m & 1)
-    // at obase + sum of on[b] over the bits of j.
-    const uint32_t tmask = (1u << d.T) - 1, nmask = tmask & ~dd.blockmask;
-    const int q4 = warp & 3, cgrp = warp >> 2;
-    const uint32_t g = tid & 7, nrow = (uint32_t)tid >> 3;
-    double sw = 0.0;   // W row scale of lane m
-    uint64_t lrow = 0, lb[3] = {0, 0, 0}, obase = 0, on[3] = {0, 0, 0};
-    bool pairs = false;   // block index bit 0 is state bit 0: amplitude pairs are 32-byte runs
-    if (!issuer) {
-        const uint32_t m = 32u * q4 + lane;
-        auto jn = [&](uint32_t v) { return pass_off(deposit_bits(v, nmask), d); };
-        auto jb = [&](uint32_t v) { return pass_off(deposit_bits(v, dd.blockmask), d); };
-        lrow = jn(nrow) + jb(8 * g);
-#pragma unroll
-        for (int b = 0; b < 3; ++b) lb[b] = jb(1u << b);
-        pairs = lb[0] == 1;
-        obase = jb(m >> 1) + jn(16u * cgrp + (m & 1u));
-#pragma unroll
-        for (int b = 0; b < 3; ++b) on[b] = jn(2u << b);
-        // W digit planes into TMEM: lanes 32 q4 .. + 31, columns 56 cgrp .. + 55
-        const uint4 *src = reinterpret_cast<const uint4 *>(gW + (size_t)m * kI8WCols + 56u * cgrp);
-#pragma unroll 1
-        for (int c8 = 0; c8 < 7; ++c8) {
-            const uint4 a = src[2 * c8], b = src[2 * c8 + 1];
-            const uint32_t taddr = tmem + ((32u * q4) << 16) + 56u * cgrp + 8u * c8;
-            asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                         "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
-                         : "memory");
-        }
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-        sw = reinterpret_cast<const double *>(gW + 128 * kI8WCols)[m];
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-
     if (issuer) {
         if (lane == 0) {
             uint32_t it = 0;
             bool stop = false;
+            const uint32_t wbase = s_u32(sW);
             for (uint64_t o = o_lo; o < o_hi && !stop && !bad_s; ++o, ++it) {
                 const uint32_t b = it & 1u;
                 if (!tc_wait(&full[b], (it >> 1) & 1u)) {
@@ -201,30 +194,31 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint32_t planes = s_u32(sm + b * kI8BufBytes);
+                const uint32_t planes = s_u32(sB + b * kI8BufBytes);
 #pragma unroll 1
                 for (int e = 0; e < kI8Weights; ++e) {   // weight wd: products (i, wd - i)
                     const int wd = kI8LowWeight + e, i0 = max(0, wd - (kI8Digits - 1));
-                    const uint32_t gg = (uint32_t)kI8Weights * it + (uint32_t)e, slot = gg & (kI8Slots - 1);
+                    const uint32_t gg = (uint32_t)kI8Weights * it + (uint32_t)e, slot = gg % kI8Slots;
                     if (gg >= (uint32_t)kI8Slots && !tc_wait(&empty[slot], ((gg / kI8Slots) - 1) & 1u)) {
                         stop = true;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t acc = tmem + kI8AccCol + 64u * slot;
+                    const uint32_t acc = tmem + 64u * slot;
 #pragma unroll 1
                     for (int i = i0; i <= min(kI8Digits - 1, wd); ++i) {
                         const int j = wd - i;
                         const uint32_t idesc = j == kI8Digits - 1 ? kI8IdescS : kI8IdescU;
+                        const uint32_t aplane = wbase + (uint32_t)i * kI8WPlaneBytes;
                         const uint32_t bplane = planes + (uint32_t)j * kI8PlaneBytes;
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk) {
                             const uint32_t en = (i != i0 || kk) ? 1u : 0u;
                             asm volatile(
                                 "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                                "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
                                     acc),
-                                "r"(tmem + 32u * i + 8u * kk), "l"(sw128_desc(bplane + 32u * kk)), "r"(idesc),
+                                "l"(sw128_desc(aplane + 32u * kk)), "l"(sw128_desc(bplane + 32u * kk)), "r"(idesc),
                                 "r"(en), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
                                 : "memory");
                         }
@@ -246,10 +240,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
         // the eight amplitudes of (row nrow, block indices 8 g ..) of supertile o
         auto load = [&](double2 (&x)[8], uint64_t o) {
             const double2 *p = s + pass_base(o, d) + lrow;
-            if (pairs) {
+            if ((lbp & 63u) == 0) {   // block index bit 0 is state bit 0: pairs are 32-byte runs
 #pragma unroll
                 for (int a = 0; a < 8; a += 2) {
-                    const double *q = reinterpret_cast<const double *>(p + ((a & 2) ? lb[1] : 0) + ((a & 4) ? lb[2] : 0));
+                    const double *q =
+                        reinterpret_cast<const double *>(p + ((a & 2) ? bitoff(lbp, 1) : 0) + ((a & 4) ? bitoff(lbp, 2) : 0));
                     double r0, r1, r2, r3;
                     asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
                                  : "=d"(r0), "=d"(r1), "=d"(r2), "=d"(r3)
@@ -260,11 +255,12 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             } else {
 #pragma unroll
                 for (int a = 0; a < 8; ++a)
-                    x[a] = p[((a & 1) ? lb[0] : 0) + ((a & 2) ? lb[1] : 0) + ((a & 4) ? lb[2] : 0)];
+                    x[a] = p[((a & 1) ? bitoff(lbp, 0) : 0) + ((a & 2) ? bitoff(lbp, 1) : 0) +
+                             ((a & 4) ? bitoff(lbp, 2) : 0)];
             }
         };
-        // registers -> seven digit planes (row nrow, K chunk g) and the row's exponent
-        auto split = [&](const double2 (&x)[8], unsigned char *planes, int *es_row) {
+        // registers -> seven digit planes (row nrow, K chunk g) and the row's scale
+        auto split = [&](const double2 (&x)[8], unsigned char *planes, double *ss_row) {
             uint32_t ek = 0;
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
@@ -275,15 +271,16 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             ek = max(ek, __shfl_xor_sync(0xffffffffu, ek, 2));
             ek = max(ek, __shfl_xor_sync(0xffffffffu, ek, 4));
             const int es = (int)(ek >> 20);
-            if (g == 0) es_row[nrow] = es;
+            // rows below 2^-959 are flushed to zero (their scale 2^(1044 - es)
+            // would not be a finite double)
+            const bool live = es >= 64;
+            const double scale = live ? __hiloint2double((2067 - es) << 20, 0) : 0.0;
+            if (g == 0) ss_row[nrow] = live ? __hiloint2double((es - 5) << 20, 0) : 0.0;
             uint32_t lo[16], hi[16];
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
-                const int64_t vr = to_fixed(x[a].x, es), vi = to_fixed(x[a].y, es);
-                lo[2 * a] = (uint32_t)(uint64_t)vr;
-                hi[2 * a] = (uint32_t)((uint64_t)vr >> 32);
-                lo[2 * a + 1] = (uint32_t)(uint64_t)vi;
-                hi[2 * a + 1] = (uint32_t)((uint64_t)vi >> 32);
+                to_fixed(x[a].x, scale, lo[2 * a], hi[2 * a]);
+                to_fixed(x[a].y, scale, lo[2 * a + 1], hi[2 * a + 1]);
             }
             uint32_t pl[kI8Digits][4];
 #pragma unroll
@@ -313,52 +310,61 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(bb);
         };
+        // int32 accumulator a -> acc += a sc, exactly on the FP64 pipe:
+        // 2^52 + (a + 2^31) has a + 2^31 as its low mantissa bits
+        auto accumulate = [&](double (&acc)[16], const uint32_t (&r)[16], double sc) {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const double a = __hiloint2double(0x43300000, (int)(r[c] ^ 0x80000000u)) - 4503601774854144.0;
+                acc[c] = fma(a, sc, acc[c]);
+            }
+        };
+        auto tmem_ld16 = [&](uint32_t taddr, uint32_t (&r)[16]) {
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                "%12, %13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+        };
         // the seven accumulators of supertile it (at o), combined and stored;
-        // false if a wait ran out
+        // false if a wait ran out.  A commit covers every earlier MMA, so the
+        // warp waits for every second weight and reads two.
         auto drain = [&](uint32_t it, uint64_t o) -> bool {
             double acc[16];
 #pragma unroll
             for (int c = 0; c < 16; ++c) acc[c] = 0.0;
+            const uint32_t lanecol = tmem + ((32u * q4) << 16) + 16u * cgrp;
 #pragma unroll 1
-            for (int e = 0; e < kI8Weights; ++e) {
-                const uint32_t gg = (uint32_t)kI8Weights * it + (uint32_t)e, slot = gg & (kI8Slots - 1);
-                if (!wait_warp(&accf[slot], (gg / kI8Slots) & 1u)) return false;
+            for (int e = 0; e < kI8Weights; e += 2) {
+                const int e1 = min(e + 1, kI8Weights - 1);
+                const uint32_t g0 = (uint32_t)kI8Weights * it + (uint32_t)e, g1 = g0 + (uint32_t)(e1 - e);
+                if (!wait_warp(&accf[g1 % kI8Slots], (g1 / kI8Slots) & 1u)) return false;
                 tc_fence_after();
-                uint32_t r[16];
-                const uint32_t taddr = tmem + ((32u * q4) << 16) + kI8AccCol + 64u * slot + 16u * cgrp;
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-                    "%12, %13, %14, %15}, [%16];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                      "=r"(r[14]), "=r"(r[15])
-                    : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                tc_fence_before();
-                arrive(&empty[slot]);
-                // weight 2^(8 (d - 12)), least significant first.  int32 ->
-                // double exactly on the FP64 pipe: 2^52 + (a + 2^31) has
-                // a + 2^31 as its low mantissa bits
-                const double sc = __hiloint2double((1023 - 96 + 8 * (kI8LowWeight + e)) << 20, 0);
-#pragma unroll
-                for (int c = 0; c < 16; ++c) {
-                    const double a = __hiloint2double(0x43300000, (int)(r[c] ^ 0x80000000u)) - 4503601774854144.0;
-                    acc[c] = fma(a, sc, acc[c]);
+                // weight 2^(8 (d - 12)) times the W row scale, least significant first
+                double sc = sw * __hiloint2double((1023 - 96 + 8 * (kI8LowWeight + e)) << 20, 0);
+                for (uint32_t gk = g0; gk <= g1; ++gk, sc *= 256.0) {
+                    uint32_t r[16];
+                    tmem_ld16(lanecol + 64u * (gk % kI8Slots), r);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    tc_fence_before();
+                    arrive(&empty[gk % kI8Slots]);
+                    accumulate(acc, r, sc);
                 }
             }
-            // scale back and store: lane pairs (re, im) of i' exchange halves
-            const int *es_row = es_s[it % 3];
+            // scale by the column and store: lane pairs (re, im) of i' exchange halves
+            const double *ss_row = ss_s[it % 3];
             const uint32_t comp = lane & 1u;
             double2 *out = s + pass_base(o, d) + obase;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const int e0 = es_row[16 * cgrp + 2 * j], e1 = es_row[16 * cgrp + 2 * j + 1];
-                const double s0 = e0 >= 6 ? __hiloint2double((e0 - 5) << 20, 0) : 0.0;
-                const double s1 = e1 >= 6 ? __hiloint2double((e1 - 5) << 20, 0) : 0.0;
-                const double v0 = acc[2 * j] * sw * s0, v1 = acc[2 * j + 1] * sw * s1;
+                const double2 sc = *reinterpret_cast<const double2 *>(ss_row + 16 * cgrp + 2 * j);
+                const double v0 = acc[2 * j] * sc.x, v1 = acc[2 * j + 1] * sc.y;
                 const double keep = comp ? v1 : v0, send = comp ? v0 : v1;
                 const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
-                const uint64_t oj = ((j & 1) ? on[0] : 0) + ((j & 2) ? on[1] : 0) + ((j & 4) ? on[2] : 0);
+                const uint64_t oj =
+                    ((j & 1) ? bitoff(onp, 0) : 0) + ((j & 2) ? bitoff(onp, 1) : 0) + ((j & 4) ? bitoff(onp, 2) : 0);
                 out[oj] = comp ? make_double2(recv, keep) : make_double2(keep, recv);
             }
             return true;
@@ -378,7 +384,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 bad = true;
                 break;
             }
-            split(x, sm + (it & 1u) * kI8BufBytes, es_s[it % 3]);
+            split(x, sB + (it & 1u) * kI8BufBytes, ss_s[it % 3]);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             arrive(&full[it & 1u]);
             if (o + 1 < o_hi) load(x, o + 1);
@@ -408,8 +414,10 @@ static int biased_exponent(double x) {
 
 // Digit planes of W = the real embedding of U: row m's entries scaled by
 // 2^(1076 - e_m) (e_m its largest biased exponent), rounded to integers and
-// written as seven balanced base-256 digits; plane i of row m at words
-// m * 224 + 32 i + k / 4 (byte k % 4), then the row scales 2^(e_m - 1028).
+// written as seven balanced base-256 digits; plane i is the A operand image
+// (128 rows of 128 bytes, K-major, 128-byte swizzle: byte k of row m at
+// 16384 i + 128 m + 16 ((k / 16) ^ (m % 8)) + k % 16), followed by the row
+// scales 2^(e_m - 1028).
 void dense_i8_operand(const DenseBlock &b, std::vector<uint32_t> &out) {
     out.assign(kI8OperandBytes / 4, 0);
     unsigned char *bytes = reinterpret_cast<unsigned char *>(out.data());
@@ -436,7 +444,9 @@ void dense_i8_operand(const DenseBlock &b, std::vector<uint32_t> &out) {
                 } else {
                     dg = (int)v;   // |v| <= 65 after six balanced digits of a 55-bit value
                 }
-                bytes[((size_t)m * kI8WCols + 32u * i + (unsigned)k / 4) * 4 + (unsigned)k % 4] = (unsigned char)(int8_t)dg;
+                const size_t off = (size_t)i * kI8WPlaneBytes + 128u * m + 16u * ((unsigned)(k >> 4) ^ (m & 7u)) +
+                                   (unsigned)(k & 15);
+                bytes[off] = (unsigned char)(int8_t)dg;
             }
         }
     }

@@ -4,8 +4,9 @@ The 30-qubit, 20-layer random U3 + brick-CZ circuit (seed 2030, the timed
 workload) is run by the unmodified reference MEM runner (oracle/_ref,
 src/MEM_Runner.cpp:101-134) on the host cores and by this engine on the GPU:
 the per-gate complex128 path must match it to 1e-12 in every one of the 2^30
-amplitudes, the fused complex128 passes as well, and the complex64
-tensor-core blocks to 1 - F <= 1e-6.  The 30-qubit QFT, written as a
+amplitudes, the fused complex128 passes and the complex128 tensor-core blocks
+(exact int8 digit products) as well, and the complex64 tensor-core blocks to
+1 - F <= 1e-6.  The 30-qubit QFT, written as a
 12-qubit-chunk subcircuit file, is run by the reference's subcircuit runner
 (src/MEM_Runner.cpp:136-185) and through qk_apply_groups.  The reference's
 16 GiB states stay in files and are compared 1 GiB at a time on the GPU.
@@ -104,6 +105,14 @@ def test_random30_fused_forms_match_reference(random30_reference):
         dmax, _ = compare(sv, ref)
         p.close()
     print(f"random-30 fused c128 passes vs reference: max |damp| = {dmax:.3e}")
+    assert dmax <= TOL_C128
+    with StateVector(N, "c128") as sv:
+        p = Plan(circ, N, "c128", fuse_width=6)
+        p.apply(sv)
+        sv.synchronize()
+        dmax, infid = compare(sv, ref)
+        p.close()
+    print(f"random-30 c128 int8 tensor-core blocks vs reference: max |damp| = {dmax:.3e}, 1 - F = {infid:.3e}")
     assert dmax <= TOL_C128
     with StateVector(N, "c64") as sv:
         p = Plan(circ, N, "c64", fuse_width=6)
