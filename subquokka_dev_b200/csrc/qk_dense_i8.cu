@@ -24,8 +24,8 @@
 //     d = i + j add up in one int32 accumulator (|sum| <= 7 x 128 x 128 x 255
 //     < 2^25);
 //   - the seven accumulators of a supertile are combined in FP64 and scaled
-//     back by 2^(e_w - 1028) 2^(e_s - 1028).  Rows whose largest entry is
-//     below 2^-1017 come out as zero.
+//     back by 2^(e_w - 1028) 2^(e_s - 1028).  State rows whose largest entry
+//     is below 2^-959 come out as zero.
 //
 // Operands and memory:
 //   - W's digit planes are the A operand in shared memory (M = 128 rows m,
@@ -116,10 +116,14 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     __shared__ __align__(8) uint64_t full[2], accf[kI8Slots], empty[kI8Slots], fin;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int bad_s;
-    // column scales 2^(e_s - 1028) of supertile it at ss_s[it % 3]: a warp
-    // writes those of supertile it + 3 only after every warp has drained the
-    // last weight of supertile it + 1, i.e. has stored supertile it
-    __shared__ __align__(16) double ss_s[3][64];
+    // row exponents e_s of supertile it at es_s[it % 4] (0: a flushed row;
+    // the drain scales by 2^(e_s - 1028)).  A warp
+    // writes those of supertile it + 4 after its drain of supertile it + 2,
+    // whose last MMAs were issued only once every warp had drained weight 5
+    // of supertile it + 1, so every warp has stored supertile it by then.
+    // (With three buffers a warp could overwrite them while another still
+    // stores supertile it: its drain of it + 1 waits only for weight 5 of it.)
+    __shared__ __align__(8) int es_s[4][64];
     const PassDesc &d = dd.p;
     unsigned char *sW = sm, *sB = sm + kI8WBytes;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             }
         };
         // registers -> seven digit planes (row nrow, K chunk g) and the row's scale
-        auto split = [&](const double2 (&x)[8], unsigned char *planes, double *ss_row) {
+        auto split = [&](const double2 (&x)[8], unsigned char *planes, int *es_row) {
             uint32_t ek = 0;
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             // would not be a finite double)
             const bool live = es >= 64;
             const double scale = live ? __hiloint2double((2067 - es) << 20, 0) : 0.0;
-            if (g == 0) ss_row[nrow] = live ? __hiloint2double((es - 5) << 20, 0) : 0.0;
+            if (g == 0) es_row[nrow] = live ? es : 0;
             uint32_t lo[16], hi[16];
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
@@ -354,13 +358,15 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 }
             }
             // scale by the column and store: lane pairs (re, im) of i' exchange halves
-            const double *ss_row = ss_s[it % 3];
+            const int *es_row = es_s[it % 4];
             const uint32_t comp = lane & 1u;
             double2 *out = s + pass_base(o, d) + obase;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const double2 sc = *reinterpret_cast<const double2 *>(ss_row + 16 * cgrp + 2 * j);
-                const double v0 = acc[2 * j] * sc.x, v1 = acc[2 * j + 1] * sc.y;
+                const int2 e2 = *reinterpret_cast<const int2 *>(es_row + 16 * cgrp + 2 * j);
+                const double s0 = e2.x ? __hiloint2double((e2.x - 5) << 20, 0) : 0.0;
+                const double s1 = e2.y ? __hiloint2double((e2.y - 5) << 20, 0) : 0.0;
+                const double v0 = acc[2 * j] * s0, v1 = acc[2 * j + 1] * s1;
                 const double keep = comp ? v1 : v0, send = comp ? v0 : v1;
                 const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
                 const uint64_t oj =
@@ -384,7 +390,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 bad = true;
                 break;
             }
-            split(x, sB + (it & 1u) * kI8BufBytes, ss_s[it % 3]);
+            split(x, sB + (it & 1u) * kI8BufBytes, es_s[it % 4]);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             arrive(&full[it & 1u]);
             if (o + 1 < o_hi) load(x, o + 1);

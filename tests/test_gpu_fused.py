@@ -249,3 +249,26 @@ def test_tensor_core_c128_wide_dynamic_range():
     ref = oracle.apply_circuit(tiny, n, circ)
     out = run_plan(n, circ, tiny, "c128", fuse_width=6)
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_tensor_core_c128_repeated_large_state():
+    # a 28-qubit state (4 GiB, 16k supertiles a block spread over every SM),
+    # the circuit applied three times over: every run must match the fused
+    # complex128 passes; a race between the kernel's pipeline stages shows
+    # up here as an error far above 1e-12
+    import torch
+    n = 28
+    circ = circuits.random_u3_cz(n, 6, 2828)
+    tc = Plan(circ, n, "c128", fuse_width=6)
+    ps = Plan(circ, n, "c128")
+    with StateVector(n, "c128") as a, StateVector(n, "c128") as b:
+        for rep in range(3):
+            tc.apply(a)
+            ps.apply(b)
+            a.synchronize()
+            b.synchronize()
+            d = float((a.as_torch() - b.as_torch()).abs().max())
+            assert d <= TOL_C128_TC, (rep, d)
+    tc.close()
+    ps.close()
+    torch.cuda.empty_cache()

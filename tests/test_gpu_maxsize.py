@@ -50,7 +50,7 @@ def circuit_and_expectations(n):
 
 
 @pytest.mark.parametrize("n,dtype,forms,tol", [
-    (33, "c128", ("per_gate", "passes"), 1e-9),            # the H literal 0.70710678118 loses ~1e-11 a gate
+    (33, "c128", ("per_gate", "passes", "tensor_cores"), 1e-9),   # the H literal 0.70710678118 loses ~1e-11 a gate
     (34, "c64", ("per_gate", "passes", "tensor_cores"), 2e-5),
 ])
 def test_largest_state(n, dtype, forms, tol):
