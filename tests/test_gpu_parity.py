@@ -165,6 +165,24 @@ def test_chunk_grouped_file_on_tensor_cores():
     assert 1 - abs(ov) ** 2 / (np.vdot(out, out).real * np.vdot(ref, ref).real) <= 1e-6
 
 
+def test_chunk_grouped_file_on_int8_tensor_cores():
+    # the same file's VSWAPs and groups as complex128 dense blocks on the int8
+    # tensor cores (exact digit products): within 1e-12 of the flat circuit
+    from subquokka_dev_b200 import Plan
+    n = 20
+    circ = circuits.random_u3_cz(n, 8, 6)
+    sub = chunk_groups(circ, n, 12)
+    init = circuits.random_state(n, 14)
+    ref = oracle.apply_circuit(init, n, circ)
+    plan = Plan(sub, n, "c128", groups=True, fuse_width=6)
+    with StateVector(n, "c128") as sv:
+        sv.upload(init)
+        plan.apply(sv)
+        out = sv.download()
+    plan.close()
+    assert np.abs(out - ref).max() <= 1e-12
+
+
 def inverse(circ):
     out = []
     for g in reversed(circ.gate_list()):
