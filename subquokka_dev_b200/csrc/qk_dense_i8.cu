@@ -55,6 +55,7 @@
 #include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_pass_device.cuh"
+#include "qk_operand.h"
 #include "qk_tc_device.cuh"
 
 namespace qk {
@@ -411,52 +412,6 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 }
 
 // ---- host side ----------------------------------------------------------------
-
-static int biased_exponent(double x) {
-    uint64_t u;
-    std::memcpy(&u, &x, 8);
-    return (int)((u >> 52) & 0x7FF);
-}
-
-// Digit planes of W = the real embedding of U: row m's entries scaled by
-// 2^(1076 - e_m) (e_m its largest biased exponent), rounded to integers and
-// written as seven balanced base-256 digits; plane i is the A operand image
-// (128 rows of 128 bytes, K-major, 128-byte swizzle: byte k of row m at
-// 16384 i + 128 m + 16 ((k / 16) ^ (m % 8)) + k % 16), followed by the row
-// scales 2^(e_m - 1028).
-void dense_i8_operand(const DenseBlock &b, std::vector<uint32_t> &out) {
-    out.assign(kI8OperandBytes / 4, 0);
-    unsigned char *bytes = reinterpret_cast<unsigned char *>(out.data());
-    double *scale = reinterpret_cast<double *>(out.data() + kI8OperandWords);
-    for (int m = 0; m < 128; ++m) {
-        const int ip = m >> 1, a = m & 1;
-        double row[128];
-        int em = 0;
-        for (int k = 0; k < 128; ++k) {
-            const int i = k >> 1, c = k & 1;
-            const double ur = b.u[2 * (ip * 64 + i)], ui = b.u[2 * (ip * 64 + i) + 1];
-            row[k] = a == 0 ? (c == 0 ? ur : -ui) : (c == 0 ? ui : ur);
-            em = std::max(em, biased_exponent(row[k]));
-        }
-        scale[m] = em > 0 ? std::ldexp(1.0, em - 1028) : 0.0;
-        if (em == 0) continue;
-        for (int k = 0; k < 128; ++k) {
-            long long v = std::llrint(std::ldexp(row[k], 1076 - em));
-            for (int i = 0; i < kI8Digits; ++i) {
-                int dg;
-                if (i < kI8Digits - 1) {
-                    dg = (int)((v + 128) & 255) - 128;
-                    v = (v - dg) / 256;
-                } else {
-                    dg = (int)v;   // |v| <= 65 after six balanced digits of a 55-bit value
-                }
-                const size_t off = (size_t)i * kI8WPlaneBytes + 128u * m + 16u * ((unsigned)(k >> 4) ^ (m & 7u)) +
-                                   (unsigned)(k & 15);
-                bytes[off] = (unsigned char)(int8_t)dg;
-            }
-        }
-    }
-}
 
 int launch_dense_i8(double2 *state, int n, const DenseDesc &dd, const uint32_t *dW, int *derr, cudaStream_t st) {
     if (n < kI8TileBits || dd.p.T != kI8TileBits || dd.p.L < 1 || __builtin_popcount(dd.blockmask) != kDenseQubits)

@@ -41,6 +41,7 @@
 #include "qk_device.h"
 #include "qk_internal.h"
 #include "qk_pass_device.cuh"
+#include "qk_operand.h"
 #include "qk_tc_device.cuh"
 
 namespace qk {
@@ -52,14 +53,6 @@ constexpr int kTcMinTileBits = 12;                    // 64 x 64
 constexpr uint32_t kTcOpBytes = 128 * 128 * 2;        // one 128 x 128 bf16 operand
 constexpr uint32_t kTcSmem = 6 * kTcOpBytes;          // W hi/lo + two state buffers hi/lo
 constexpr uint32_t kTcTmemCols = 256;                 // two 128-column accumulators
-
-// Byte offset of element (row r, k) of a 128-row x 128-K bf16 operand in the
-// canonical K-major 128-byte-swizzle layout: two K atoms of 64 elements (16 KB
-// each, row r at 128 r), the 16-byte chunk index XORed with r % 8 so that
-// eight rows' chunks at one K fall into different banks.
-__host__ __device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t k) {
-    return (k >> 6) * 16384u + r * 128u + ((((k >> 3) & 7u) ^ (r & 7u)) << 4) + (k & 7u) * 2u;
-}
 
 // Shared-memory descriptor of MMA step kk (K = 16 kk .. 16 kk + 15) of an
 // operand at saddr (1024-byte aligned): the step's 32 bytes inside its atom.
@@ -415,65 +408,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2 *__restrict__
 }
 
 // ---- host side ----------------------------------------------------------------
-
-static uint16_t bf16_rn(float x) {
-    uint32_t u;
-    std::memcpy(&u, &x, 4);
-    const uint32_t lsb = (u >> 16) & 1u;
-    u += 0x7FFFu + lsb;
-    return (uint16_t)(u >> 16);
-}
-static float bf16_to_f(uint16_t h) {
-    const uint32_t u = (uint32_t)h << 16;
-    float f;
-    std::memcpy(&f, &u, 4);
-    return f;
-}
-
-// W = real embedding of U (rows/cols interleaved re/im), split into bf16 hi +
-// lo, each in the canonical K-major layout: 2 x 32 KiB.
-void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out) {
-    out.assign(2 * 128 * 128, 0);
-    unsigned char *hi = reinterpret_cast<unsigned char *>(out.data());
-    unsigned char *lo = hi + kTcOpBytes;
-    for (int ip = 0; ip < 64; ++ip)
-        for (int i = 0; i < 64; ++i) {
-            const double ur = b.u[2 * (ip * 64 + i)], ui = b.u[2 * (ip * 64 + i) + 1];
-            const double v[2][2] = {{ur, -ui}, {ui, ur}};
-            for (int a = 0; a < 2; ++a)
-                for (int c = 0; c < 2; ++c) {
-                    const float x = (float)v[a][c];
-                    const uint16_t h = bf16_rn(x);
-                    const uint16_t l = bf16_rn((float)(v[a][c] - (double)bf16_to_f(h)));
-                    const uint32_t off = sw128_off(2 * ip + a, 2 * i + c);
-                    std::memcpy(hi + off, &h, 2);
-                    std::memcpy(lo + off, &l, 2);
-                }
-        }
-}
-
-// tile bits of a block: its six qubits plus the lowest other state bits, up
-// to max_tile_bits (13: 64 x 128 supertiles)
-DenseDesc dense_block_desc(const DenseBlock &b, int n, int max_tile_bits) {
-    DenseDesc dd;
-    std::memset(&dd, 0, sizeof dd);
-    std::vector<char> in(n, 0);
-    for (int k = 0; k < kDenseQubits; ++k) in[b.q[k]] = 1;
-    const int tbits = std::min(n, max_tile_bits);
-    int cnt = kDenseQubits;
-    for (int q = 0; q < n && cnt < tbits; ++q)
-        if (!in[q]) { in[q] = 1; ++cnt; }
-    int t = 0;
-    for (int q = 0; q < n; ++q)
-        if (in[q]) {
-            for (int k = 0; k < kDenseQubits; ++k)
-                if (b.q[k] == q) dd.blockmask |= 1u << t;
-            dd.p.bpos[t++] = q;
-        }
-    dd.p.T = t;
-    while (dd.p.L < dd.p.T && dd.p.bpos[dd.p.L] == dd.p.L) ++dd.p.L;
-    return dd;
-}
 
 template <int NROWS, bool STATE_N>
 static int launch_dense_tc_n(float2 *state, int n, const DenseDesc &dd, const uint16_t *dW, int *derr,

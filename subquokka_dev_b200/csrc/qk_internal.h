@@ -186,6 +186,8 @@ constexpr int kI8Digits = 7;
 constexpr size_t kI8OperandWords = 128 * 32 * kI8Digits;
 constexpr size_t kI8OperandBytes = kI8OperandWords * 4 + 128 * sizeof(double);
 void dense_i8_operand(const DenseBlock &b, std::vector<uint32_t> &out);   // kI8OperandBytes / 4 words
+// complex64 blocks (qk_dense_tc.cu): W split into bf16 hi and lo operands
+void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out);   // 2 x 128 x 128
 // Bytes of one block's device operand for dtype.
 size_t dense_operand_bytes(int dtype);
 // Backward sweep of an adjoint gradient: the inverses of gates[ng-1..0] on

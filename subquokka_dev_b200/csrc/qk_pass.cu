@@ -326,7 +326,6 @@ int run_plan_at(void *state, int dtype, const HostPlan &hp, const TOp *ops, cons
 using namespace qk;
 
 namespace qk {
-void dense_block_operand(const DenseBlock &b, std::vector<uint16_t> &out);
 // the blocks of a dense plan in order (qk_dense_tc.cu)
 int run_dense_blocks(void *state, int n, int dtype, const std::vector<DenseBlock> &blocks, const void *dA, int *derr,
                      cudaStream_t st);

@@ -22,6 +22,7 @@
 // with H (the reference's H constant is 1.1e-11 off unitary, and gradient
 // ops move past gates on other qubits).  Exit status 0 on success.
 #include "dense_sim.h"
+#include "qk_operand.h"
 
 using namespace dense_sim;
 using qk::HostPlan;
@@ -29,6 +30,66 @@ using qk::PassDesc;
 using qk::TOp;
 
 namespace {
+
+float bf16_value(uint16_t h) {
+    const uint32_t u = (uint32_t)h << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// The tensor-core operands of block b against its unitary: the complex128
+// digit planes rebuild every entry of the real embedding W to half a unit
+// of its row's last digit, every digit is in range; the complex64 bf16 hi +
+// lo pair rebuilds W to bf16 x bf16 rounding; the supertile layouts hold the
+// block's qubits and the lowest others, ascending.
+int check_operands(const qk::DenseBlock &b, int n) {
+    int bad = 0;
+    std::vector<uint32_t> w8;
+    qk::dense_i8_operand(b, w8);
+    const unsigned char *digits = reinterpret_cast<const unsigned char *>(w8.data());
+    const double *scale = reinterpret_cast<const double *>(w8.data() + qk::kI8OperandWords);
+    std::vector<uint16_t> w16;
+    qk::dense_block_operand(b, w16);
+    const unsigned char *hi = reinterpret_cast<const unsigned char *>(w16.data());
+    const unsigned char *lo = hi + qk::kBf16OperandBytes;
+    double e8 = 0, e16 = 0;
+    for (int m = 0; m < 128; ++m)
+        for (int k = 0; k < 128; ++k) {
+            const int ip = m >> 1, a = m & 1, i = k >> 1, c = k & 1;
+            const double ur = b.u[2 * (ip * 64 + i)], ui = b.u[2 * (ip * 64 + i) + 1];
+            const double w = a == 0 ? (c == 0 ? ur : -ui) : (c == 0 ? ui : ur);
+            double v = 0;
+            for (int d = qk::kI8Digits - 1; d >= 0; --d) {
+                const int dg = (int8_t)digits[qk::sw128_i8_off((uint32_t)d, (uint32_t)m, (uint32_t)k)];
+                if (d < qk::kI8Digits - 1 ? (dg < -128 || dg > 127) : (dg < -65 || dg > 65)) ++bad;
+                v = v * 256 + dg;
+            }
+            // scale[m] = 2^(e_m - 1028); one unit of v is 2^(e_m - 1076)
+            const double unit = std::ldexp(scale[m], -48);
+            e8 = std::max(e8, std::fabs(v * unit - w) / unit);
+            uint16_t h, l;
+            std::memcpy(&h, hi + qk::sw128_off((uint32_t)m, (uint32_t)k), 2);
+            std::memcpy(&l, lo + qk::sw128_off((uint32_t)m, (uint32_t)k), 2);
+            e16 = std::max(e16, std::fabs((double)bf16_value(h) + (double)bf16_value(l) - w));
+        }
+    if (e8 > 0.5 || e16 > 1e-4) {
+        std::printf("operands: digit error %.3g units, bf16 error %.3g\n", e8, e16);
+        ++bad;
+    }
+    for (int tb : {12, 13}) {
+        const qk::DenseDesc dd = qk::dense_block_desc(b, n, tb);
+        int blockbits = 0;
+        for (int t = 0; t < dd.p.T; ++t) {
+            if (t && dd.p.bpos[t] <= dd.p.bpos[t - 1]) ++bad;
+            const bool inblock = std::find(b.q, b.q + qk::kDenseQubits, dd.p.bpos[t]) != b.q + qk::kDenseQubits;
+            if (inblock != (((dd.blockmask >> t) & 1u) != 0)) ++bad;
+            blockbits += inblock;
+        }
+        if (dd.p.T != std::min(n, tb) || blockbits != qk::kDenseQubits || dd.p.L < 1) ++bad;
+    }
+    return bad;
+}
 
 int bit_of(uint8_t code, uint64_t j, uint64_t base) {
     if (code == qk::kNoQubit) return -1;
@@ -255,6 +316,7 @@ int main() {
             }
             for (const qk::DenseBlock &b : blocks) {
                 std::vector<int> qs;
+                if (!b.perm) bad += check_operands(b, 14);   // layouts of these qubits in a 14-qubit state
                 if (b.perm) {
                     const auto m = matrix_of(b.perm_op, qs);
                     apply_matrix(have, n, qs, m);

@@ -39,4 +39,4 @@ def test_rewrites_keep_states_and_gradients(tmp_path):
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="g++ absent")
 def test_plans_compute_the_circuit(tmp_path):
-    build_and_run(tmp_path, "plan_check.cpp", ["qk_plan.cpp", "qk_rewrite.cpp", "qk_parse.cpp"])
+    build_and_run(tmp_path, "plan_check.cpp", ["qk_plan.cpp", "qk_rewrite.cpp", "qk_parse.cpp", "qk_dense_host.cpp"])
