@@ -498,12 +498,18 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
                 case 3: g = reg_grad<3>(v, w, op.b, gc, &g2); break;
                 case 4: g = reg_grad<4>(v, w, op.b, gc, &g2); break;
                 }
+                // a tile of fewer than 32 threads (2^(T - r) < 32) is a
+                // partial warp: the shuffles stay within its lanes
+                const uint32_t nl = blockDim.x < 32 ? blockDim.x : 32;
+                const uint32_t lanes = nl == 32 ? 0xffffffffu : (1u << nl) - 1;
 #pragma unroll
-                for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+                for (uint32_t o = 16; o; o >>= 1)
+                    if (o < nl) g += __shfl_xor_sync(lanes, g, (int)o);
                 if ((tid & 31) == 0) atomicAdd(gsm + (op.bits[0] | (op.bits[1] << 8)), (double)g);
                 if (op.b == 5) {
 #pragma unroll
-                    for (int o = 16; o; o >>= 1) g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+                    for (uint32_t o = 16; o; o >>= 1)
+                        if (o < nl) g2 += __shfl_xor_sync(lanes, g2, (int)o);
                     if ((tid & 31) == 0) atomicAdd(gsm + (op.bits[2] | (op.bits[3] << 8)), (double)g2);
                 }
             }

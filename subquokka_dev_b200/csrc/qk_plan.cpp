@@ -45,14 +45,15 @@ PlanOptions default_plan_options(int dtype, int n) {
     return o;
 }
 
-// Two-state (adjoint) passes hold twice the data per thread and per tile:
-// 1024-amplitude tiles (complex128) / 2048 (complex64), 8 amplitudes a
-// thread.  On the 26-qubit HEA this is 177 against 190 ms (complex128, 2048-
-// amplitude tiles) and 115 against 117 ms (complex64, 4096).
+// Two-state (adjoint) passes: small tiles, 256 amplitudes (complex128) / 512
+// (complex64) with 8 a thread, so that many CTAs share an SM.  On the
+// 26-qubit HEA (12 layers, 624 parameters): complex128 178 ms against 183 ms
+// with 1024-amplitude tiles and 190 ms with 2048; complex64 113 ms against
+// 117 ms with 2048 or 4096 (measured in one run each).
 PlanOptions default_adjoint_options(int dtype, int n) {
     PlanOptions o;
     o.dtype = dtype;
-    o.tile_bits = std::min(n, dtype == QK_C128 ? 10 : 11);
+    o.tile_bits = std::min(n, dtype == QK_C128 ? 8 : 9);
     o.reg_bits = std::min(o.tile_bits, 3);
     return o;
 }
