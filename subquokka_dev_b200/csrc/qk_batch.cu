@@ -707,7 +707,7 @@ int qk_batch_create(int ncirc, const int32_t *nqubits, const qk_gate *gates, con
         struct Cand { int T, r; };
         const std::vector<Cand> fc = b->dtype == QK_C64 ? std::vector<Cand>{{11, 4}, {12, 3}, {12, 4}, {13, 4}}
                                                         : std::vector<Cand>{{11, 4}, {12, 3}, {11, 3}};
-        const std::vector<Cand> bc = b->dtype == QK_C64 ? std::vector<Cand>{{11, 3}, {12, 3}}
+        const std::vector<Cand> bc = b->dtype == QK_C64 ? std::vector<Cand>{{10, 3}, {11, 3}, {12, 3}}
                                                         : std::vector<Cand>{{11, 3}, {11, 2}, {10, 2}};
         float best = 1e30f;
         PlanOptions bf = b->fo, bb = b->bo;
