@@ -214,6 +214,9 @@ static int launch_pass(C *s, int n, int r, const PassDesc &d, const TOp *ops, co
         case 2: return launch_pass_r<C, 4, 2>(a, n, d, st);
         case 3:
             return launch_pass_r<C, 8, 2>(a, n, d, st);
+        case 4:
+            if constexpr (sizeof(C) == sizeof(float2)) return launch_pass_r<C, 16, 2>(a, n, d, st);
+            break;
         }
         return fail(QK_ERR_ARG, "reg_bits %d unsupported for two-state passes", r);
     }

@@ -45,16 +45,17 @@ PlanOptions default_plan_options(int dtype, int n) {
     return o;
 }
 
-// Two-state (adjoint) passes: small tiles, 256 amplitudes (complex128) / 512
-// (complex64) with 8 a thread, so that many CTAs share an SM.  On the
-// 26-qubit HEA (12 layers, 624 parameters): complex128 178 ms against 183 ms
-// with 1024-amplitude tiles and 190 ms with 2048; complex64 113 ms against
-// 117 ms with 2048 or 4096 (measured in one run each).
+// Two-state (adjoint) passes.  complex128: small tiles, 256 amplitudes with
+// 8 a thread, so that many CTAs share an SM; on the 26-qubit HEA (12 layers,
+// 624 parameters) 178 ms against 183 ms with 1024-amplitude tiles and 190 ms
+// with 2048.  complex64: 2048-amplitude tiles with 16 amplitudes of each
+// state a thread (254 registers), 106.5 ms there against 113 ms with 512-
+// amplitude tiles and 8 a thread, 109 / 111 ms with 1024 / 4096 and 16.
 PlanOptions default_adjoint_options(int dtype, int n) {
     PlanOptions o;
     o.dtype = dtype;
-    o.tile_bits = std::min(n, dtype == QK_C128 ? 8 : 9);
-    o.reg_bits = std::min(o.tile_bits, 3);
+    o.tile_bits = std::min(n, dtype == QK_C128 ? 8 : 11);
+    o.reg_bits = std::min(o.tile_bits, dtype == QK_C128 ? 3 : 4);
     return o;
 }
 
@@ -598,7 +599,9 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
                        HostPlan &plan) {
     int rc = check_options(o, n);
     if (rc) return rc;
-    if (o.reg_bits > 3) return fail(QK_ERR_ARG, "adjoint passes take at most 3 register bits (two states a thread)");
+    if (o.reg_bits > (o.dtype == QK_C64 ? 4 : 3))
+        return fail(QK_ERR_ARG, "adjoint passes take at most %d register bits (two states a thread)",
+                    o.dtype == QK_C64 ? 4 : 3);
     if (o.dtype == QK_C128 && o.reg_bits == 3 && o.tile_bits - o.reg_bits > 8)
         return fail(QK_ERR_ARG, "complex128 adjoint passes with reg_bits 3 need tile_bits - reg_bits <= 8");
     std::vector<Op> fwd;
