@@ -272,3 +272,29 @@ def test_tensor_core_c128_repeated_large_state():
     tc.close()
     ps.close()
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("form", ["per_gate", "passes_c128", "tensor_core_c128", "tensor_core_c64"])
+def test_known_answers_every_form(form):
+    # the analytic answers the reference's own circuits have, through every
+    # form: H^n |0> = 0.70710678118^n everywhere (the reference's literal),
+    # RX(pi)^n |0> = (-i)^n |1...1>, QFT |0> uniform
+    n = 14
+    cases = [
+        (Circuit([make_gate("H", [q]) for q in range(n)]), lambda s: np.full_like(s, 0.70710678118 ** n)),
+        (Circuit([make_gate("RX", [q], np.pi) for q in range(n)]),
+         lambda s: np.where(np.arange(s.size) == s.size - 1, (-1j) ** n, 0)),
+        (circuits.qft(n), lambda s: np.full_like(s, 0.70710678118 ** n)),
+    ]
+    dtype = "c64" if form.endswith("c64") else "c128"
+    tol = 1e-6 if dtype == "c64" else 1e-12
+    for circ, want in cases:
+        with StateVector(n, dtype) as sv:
+            if form == "per_gate":
+                sv.apply(circ)
+            else:
+                plan = Plan(circ, n, dtype, fuse_width=6 if form.startswith("tensor") else 0)
+                plan.apply(sv)
+                plan.close()
+            out = sv.download()
+        assert np.abs(out - want(out)).max() <= tol, form
