@@ -724,12 +724,23 @@ def our_arm(args, rank, world):
                 "kernel_gbs": {k: (2 * S if k.startswith("k_dense1") else S // 2) / (statistics.mean(v) / 1e3) / 1e9
                                for k, v in per_kernel.items()}}
     launches = args.steps * (circ.ngates + 1)
-    variants = {} if args.no_fused else fused_variants(args, circ, sv, ms_per_step, alg)
-    extra = {} if (args.no_extra or rank != 0) else None
+    # the fused forms and the other workloads are single-GPU measurements:
+    # a run on N > 1 GPUs (replicas of the timed step) skips them and runs
+    # the two multi-GPU legs instead, so that it holds the GPUs briefly
+    variants = {} if (args.no_fused or world > 1) else fused_variants(args, circ, sv, ms_per_step, alg)
+    extra = {} if (args.no_extra or rank != 0 or world > 1) else None
     sharded = sharded_st = None
     if world > 1 and not args.no_extra:
-        sharded = sharded_batch(world)   # every rank takes part
-        sharded_st = sharded_state(world, args.layers)
+        # every rank takes part; an error raised on every rank alike is
+        # recorded instead of ending the run
+        try:
+            sharded = sharded_batch(world)
+        except Exception as exc:
+            sharded = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+        try:
+            sharded_st = sharded_state(world, args.layers)
+        except Exception as exc:
+            sharded_st = {"error": f"{type(exc).__name__}: {exc}"[:300]}
 
     # end to end through the public API: host gate records in, final state out to pinned host memory
     e2e = None
@@ -843,7 +854,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
         return our_arm(args, rank, world)
     finally:
