@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(pass_max_threads<C, R, NS>()) k_pass_batch(con
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
-        run_program<C, R, NS>(tl, tw, base, sd, prog, coef, gsm, N);
+        run_program<C, R, NS, false>(tl, tw, base, sd, prog, coef, gsm, N);
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < R; ++u) {
@@ -695,6 +695,8 @@ int qk_batch_create(int ncirc, const int32_t *nqubits, const qk_gate *gates, con
     }
     b->fo = default_plan_options(b->dtype, nmin);
     b->bo = default_adjoint_options(b->dtype, nmin);
+    // one kernel instance for all circuits: programs without real-op forms
+    b->fo.plain_ops = b->bo.plain_ops = 1;
     if (b->dtype == QK_C64) {
         // the batch's many small states: 1024-amplitude adjoint tiles with 8
         // amplitudes a thread (256 circuits of 14-22 qubits: 261 ms against

@@ -85,7 +85,19 @@ enum TOpKind : uint8_t {
     TOP_GRAD = 5,   // two-state passes: gacc[coef] += Im <lambda|G|psi>, G = X/Y/Z (b = 1/2/3) on slot a
     TOP_CX = 6,     // swap register slot a's pairs where qubit code b is 1 (controlled X)
     TOP_CG1 = 7,    // dense 2x2 on slot a: coef[0..3] or coef[4..7] by qubit code b (not a register slot)
+    TOP_R1 = 8,     // real 2x2 on slot a: coef[0] = (m00, m01), coef[1] = (m10, m11)
+    TOP_R2 = 9,     // real 4x4 on slots a < b (index bit0 = a): coef[2 r + h] = (m[r][2h], m[r][2h + 1])
 };
+// The kernel instance for passes marked xops carries factors that are the
+// same for all of a thread's amplitudes (TOP_DIAG / TOP_PHASE on qubits
+// outside the register slots) as one pending scalar, applied before the
+// tile is re-distributed or stored -- except where the register amplitudes
+// take 256 bytes or more (complex128 with 16 a thread, two states of 8
+// complex128 or 16 complex64): those kernels run at their register limit,
+// and the scalar's registers cost spills.
+constexpr bool pending_scalar_ok(int amp_bytes, int reg_amps, int nstates) {
+    return amp_bytes * reg_amps * nstates < 256;
+}
 
 // Qubit codes of TOP_DIAG / TOP_PHASE: < 0x80 tile-local bit; 0x80 | q global
 // qubit q that is not a tile bit (constant over a tile); 0xFF no qubit (bit =
@@ -113,6 +125,8 @@ struct PassDesc {
     int32_t perm;                 // 1: a qubit-permutation pass (VSWAP), prog unused
     int32_t nperm;
     int32_t perm_a[6], perm_b[6]; // tile-local bit pairs swapped on store (perm passes)
+    int32_t xops;                 // 1: the program has real or diagonal ops (TOP_R1, TOP_R2, TOP_DIAG,
+                                  // TOP_PHASE), run by the kernel instance that specialises them
 };
 
 // Host plan: passes + programs + complex coefficient pool (FP64).
@@ -132,6 +146,8 @@ struct PlanOptions {
     int dtype;
     int tile_bits;   // T
     int reg_bits;    // r
+    int plain_ops = 0;    // 1: no TOP_R1 / TOP_R2 (real ops as TOP_G1 / TOP_G2) and no pass marked
+                          // xops (plans of the batched kernel, which has one instance)
 };
 
 // Build a fused plan for a flat gate list (greedy tile-bit choice).
@@ -144,7 +160,8 @@ void as_matrix(const Op &op, double (&m)[8]);
 void mat2_mul(const double (&x)[8], const double (&y)[8], double (&z)[8]);
 void asap_order(std::vector<Op> &ops, int n);
 void merge_one_qubit_runs(std::vector<Op> &ops, int n);
-void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n);
+void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n, bool keep_real = false);
+bool op_is_real(const Op &op);
 void hoist_gradients(std::vector<Op> &ops, int n);
 void pair_gradients(std::vector<Op> &ops);
 void relabel_perms(std::vector<Op> &ops, int n, int L, int max_bits, int max_pairs, bool swaps);

@@ -29,7 +29,7 @@ namespace qk {
 // NS = 2 runs an adjoint pass over psi (s) and lambda (s2) together; the
 // gradient accumulators of the pass live in shared memory and are added to
 // ggrad[gparams[grad0 + i]] once per CTA.
-template <typename C, int R, int NS, bool NARROW>
+template <typename C, int R, int NS, bool NARROW, bool XOPS>
 __global__ void __launch_bounds__(NARROW ? 128 : pass_max_threads<C, R, NS>(), NARROW ? 3 : 1) k_pass(C *__restrict__ s, C *__restrict__ s2, uint64_t ntiles,
                                                        const __grid_constant__ PassDesc d, const TOp *__restrict__ gprog,
                                                        const C *__restrict__ gcoef, const int32_t *__restrict__ gparams,
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(NARROW ? 128 : pass_max_threads<C, R, NS>(), N
             }
             prefetch_tile<C, R, LOG2R>(nx, s, bn, ta);
         }
-        run_program<C, R, NS>(tl, tw, base, d, prog, coef, gsm, N);
+        run_program<C, R, NS, XOPS>(tl, tw, base, d, prog, coef, gsm, N);
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < R; ++u) {
@@ -149,7 +149,7 @@ template <typename C> struct PassArgs {
     double *ggrad;           // gradient accumulators (two-state passes)
 };
 
-template <typename C, int R, int NS, bool NARROW>
+template <typename C, int R, int NS, bool NARROW, bool XOPS>
 static int launch_pass_k(const PassArgs<C> &a, int n, const PassDesc &d, uint32_t threads, cudaStream_t st) {
     static std::atomic<uint64_t> smem_done{0};
     const size_t tile = (sizeof(C) << d.T) * NS;
@@ -157,15 +157,15 @@ static int launch_pass_k(const PassArgs<C> &a, int n, const PassDesc &d, uint32_
     const size_t smem = tile * nbuf + d.nprog * sizeof(TOp) + d.ncoef * sizeof(C) + (NS == 2 ? d.ngrad * sizeof(double) : 0);
     if (smem > (220u << 10)) return fail(QK_ERR_ARG, "pass needs %zu bytes of shared memory", smem);
     cudaError_t e;
-    e = smem_limit_once(smem_done, (const void *)k_pass<C, R, NS, NARROW>, 220 << 10);
+    e = smem_limit_once(smem_done, (const void *)k_pass<C, R, NS, NARROW, XOPS>, 220 << 10);
     if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(k_pass)");
     const int sms = device_sms();
     int mb = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass<C, R, NS, NARROW>, (int)threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb, k_pass<C, R, NS, NARROW, XOPS>, (int)threads, smem);
     if (e != cudaSuccess || mb < 1) mb = 1;
     const uint64_t ntiles = 1ull << (n - d.T);
     const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sms * mb);
-    k_pass<C, R, NS, NARROW><<<grid, threads, smem, st>>>(a.s, a.s2, ntiles, d, a.ops, a.coef, a.gparams, a.ggrad, nbuf);
+    k_pass<C, R, NS, NARROW, XOPS><<<grid, threads, smem, st>>>(a.s, a.s2, ntiles, d, a.ops, a.coef, a.gparams, a.ggrad, nbuf);
     e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_err(e, "k_pass launch");
 }
@@ -175,9 +175,16 @@ static int launch_pass_r(const PassArgs<C> &a, int n, const PassDesc &d, cudaStr
     const uint32_t threads = d.perm ? std::max<uint32_t>(1, std::min<uint32_t>(kPassThreads, 1u << d.T))
                                     : (uint32_t)((1u << d.T) / R);
     if (threads > kPassThreads || threads == 0) return fail(QK_ERR_ARG, "pass of %d tile bits needs %u threads", d.T, threads);
+    // programs with real or diagonal ops run on the instance that
+    // specialises them; the others on one without that code, whose register
+    // allocation it would otherwise change (the 30-qubit random circuit and
+    // HEA forward passes, which have neither, 1-2.5 % slower with it)
     if constexpr (pass_narrow_ok<C, R, NS>())
-        if (!d.perm && threads <= 128) return launch_pass_k<C, R, NS, true>(a, n, d, threads, st);
-    return launch_pass_k<C, R, NS, false>(a, n, d, threads, st);
+        if (!d.perm && threads <= 128)
+            return d.xops ? launch_pass_k<C, R, NS, true, true>(a, n, d, threads, st)
+                          : launch_pass_k<C, R, NS, true, false>(a, n, d, threads, st);
+    return d.xops ? launch_pass_k<C, R, NS, false, true>(a, n, d, threads, st)
+                  : launch_pass_k<C, R, NS, false, false>(a, n, d, threads, st);
 }
 
 template <typename C>

@@ -79,6 +79,76 @@ __device__ __forceinline__ void reg_g1(C (&v)[R], const C m0, const C m1, const 
     }
 }
 
+// Real 2x2 on register slot S: c0 = (m00, m01), c1 = (m10, m11); two
+// multiply-adds a component instead of the complex 2x2's four.
+template <int S, typename C, int R>
+__device__ __forceinline__ void reg_r1(C (&v)[R], const C c0, const C c1) {
+    if constexpr ((1 << S) < R) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (k & (1 << S)) continue;
+            const C a = v[k], b = v[k | (1 << S)];
+            v[k].x = fma(c0.x, a.x, c0.y * b.x);
+            v[k].y = fma(c0.x, a.y, c0.y * b.y);
+            v[k | (1 << S)].x = fma(c1.x, a.x, c1.y * b.x);
+            v[k | (1 << S)].y = fma(c1.x, a.y, c1.y * b.y);
+        }
+    }
+}
+
+// Real 4x4 on register slots A < B (index bit 0 = A): m[2 r + h] =
+// (row r's entries 2h, 2h + 1).
+template <int A, int B, typename C, int R>
+__device__ __forceinline__ void reg_r2(C (&v)[R], const C *__restrict__ m) {
+    if constexpr (A < B && (1 << B) < R) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (k & ((1 << A) | (1 << B))) continue;
+            const int k1 = k | (1 << A), k2 = k | (1 << B), k3 = k | (1 << A) | (1 << B);
+            const C x0 = v[k], x1 = v[k1], x2 = v[k2], x3 = v[k3];
+            C y[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const C p = m[2 * r], q = m[2 * r + 1];
+                y[r].x = fma(p.x, x0.x, fma(p.y, x1.x, fma(q.x, x2.x, q.y * x3.x)));
+                y[r].y = fma(p.x, x0.y, fma(p.y, x1.y, fma(q.x, x2.y, q.y * x3.y)));
+            }
+            v[k] = y[0];
+            v[k1] = y[1];
+            v[k2] = y[2];
+            v[k3] = y[3];
+        }
+    }
+}
+
+// Phase on the register elements whose bit S (and bit T) is set.
+template <int S, typename C, int R>
+__device__ __forceinline__ void reg_phase1(C (&v)[R], const C ph) {
+    if constexpr ((1 << S) < R) {
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+            if (k & (1 << S)) v[k] = cmul(v[k], ph);
+    }
+}
+template <int S, int T, typename C, int R>
+__device__ __forceinline__ void reg_phase2(C (&v)[R], const C ph) {
+    if constexpr ((1 << S) < R && (1 << T) < R) {
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+            if ((k & (1 << S)) && (k & (1 << T))) v[k] = cmul(v[k], ph);
+    }
+}
+
+// Every register amplitude of the thread (both states) times f.
+template <typename C, int R, int NW>
+__device__ __forceinline__ void scale_regs(C (&v)[R], C (&w)[NW], const C f) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        v[k] = cmul(v[k], f);
+        if constexpr (NW == R) w[k] = cmul(w[k], f);
+    }
+}
+
 // Controlled X on register slot S: swap the pair (k, k | 2^S) where bit k of
 // M (the control's value at register index k) is set.
 template <int S, typename C, int R>
@@ -356,7 +426,7 @@ __device__ __forceinline__ auto reg_grad(const C (&v)[R], const C (&w)[R], int g
 // Run a pass program on one tile (NS = 1) or on the matching tiles of two
 // states (NS = 2: psi in tl/v, lambda in tw/w; every gate acts on both and
 // TOP_GRAD accumulates Im<lambda|G|psi> into gsm).
-template <typename C, int R, int NS>
+template <typename C, int R, int NS, bool XOPS>
 __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const PassDesc &d, const TOp *prog,
                                             const C *coef, double *gsm, uint32_t N) {
     constexpr int LOG2R = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
@@ -367,10 +437,26 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
     uint32_t sb[LOG2R];  // swz of each register slot's tile bit
     uint32_t tb = 0, stb = 0;
     bool mapped = false;
+    // factor common to all of the thread's amplitudes (diagonal ops on
+    // qubits outside the register slots), applied before they leave the
+    // registers
+    constexpr bool PEND = XOPS && pending_scalar_ok((int)sizeof(C), R, NS);
+    C pend;
+    pend.x = 1;
+    pend.y = 0;
+    bool pending = false;
     for (int p = 0; p < d.nprog; ++p) {
         const TOp op = prog[p];
         switch (op.kind) {
         case TOP_REMAP: {
+            if constexpr (PEND) {
+                if (pending) {
+                    scale_regs(v, w, pend);
+                    pend.x = 1;
+                    pend.y = 0;
+                    pending = false;
+                }
+            }
             if (mapped) {
 #pragma unroll
                 for (int kk = 0; kk < R; ++kk) {
@@ -412,6 +498,35 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             }
             break;
         }
+        case TOP_R1:
+        case TOP_R2:
+            if constexpr (XOPS) {
+                if (op.kind == TOP_R1) {
+                    const C c0 = coef[op.coef], c1 = coef[op.coef + 1];
+                    switch (op.a) {
+#define QK_R1(S)                                     \
+    case S:                                          \
+        reg_r1<S>(v, c0, c1);                        \
+        if constexpr (NS == 2) reg_r1<S>(w, c0, c1); \
+        break;
+                    QK_R1(0) QK_R1(1) QK_R1(2) QK_R1(3) QK_R1(4)
+#undef QK_R1
+                    }
+                } else {
+                    const C *m = coef + op.coef;
+                    switch (op.a * 8 + op.b) {
+#define QK_R2(A, B)                                     \
+    case A * 8 + B:                                     \
+        reg_r2<A, B>(v, m);                             \
+        if constexpr (NS == 2) reg_r2<A, B>(w, m);      \
+        break;
+                    QK_R2(0, 1) QK_R2(0, 2) QK_R2(0, 3) QK_R2(0, 4) QK_R2(1, 2)
+                    QK_R2(1, 3) QK_R2(1, 4) QK_R2(2, 3) QK_R2(2, 4) QK_R2(3, 4)
+#undef QK_R2
+                    }
+                }
+            }
+            break;
         case TOP_G2: {
             const C *m = coef + op.coef;
             switch (op.a * 8 + op.b) {
@@ -455,7 +570,15 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             C p0, p1;
             if (sa >= 0) { p0 = bb ? d2 : d0; p1 = bb ? d3 : d1; }
             else if (sb >= 0) { p0 = ba ? d1 : d0; p1 = ba ? d3 : d2; }
-            else { p0 = p1 = ba ? (bb ? d3 : d1) : (bb ? d2 : d0); }
+            else {
+                // the same factor for all of the thread's amplitudes
+                p0 = p1 = ba ? (bb ? d3 : d1) : (bb ? d2 : d0);
+                if constexpr (PEND) {
+                    pend = cmul(pend, p0);
+                    pending = true;
+                    break;
+                }
+            }
             switch (sl) {
 #define QK_D1(S)                                       \
     case S:                                            \
@@ -497,19 +620,72 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
             break;
         }
         case TOP_PHASE: {
-            const C ph = coef[op.coef];
-            const uint32_t M = bit_set_at(op.a, op.bits[0], 1, base, tb) & bit_set_at(op.b, op.bits[1], 1, base, tb);
-            if (!(M & ((R >= 32) ? 0xFFFFFFFFu : ((1u << R) - 1)))) break;
+            if constexpr (!XOPS) {
+                const C ph = coef[op.coef];
+                const uint32_t M = bit_set_at(op.a, op.bits[0], 1, base, tb) & bit_set_at(op.b, op.bits[1], 1, base, tb);
+                if (!(M & ((R >= 32) ? 0xFFFFFFFFu : ((1u << R) - 1)))) break;
 #pragma unroll
-            for (int kk = 0; kk < R; ++kk)
-                if ((M >> kk) & 1) {
-                    v[kk] = cmul(v[kk], ph);
-                    if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
+                for (int kk = 0; kk < R; ++kk)
+                    if ((M >> kk) & 1) {
+                        v[kk] = cmul(v[kk], ph);
+                        if constexpr (NS == 2) w[kk] = cmul(w[kk], ph);
+                    }
+                break;
+            } else {
+                const C ph = coef[op.coef];
+                uint32_t ba, bb;
+                const int sa = code_slot_at(op.a, op.bits[0], base, tb, &ba);
+                const int sb = code_slot_at(op.b, op.bits[1], base, tb, &bb);
+                if (op.a == kNoQubit) ba = 1;
+                if (op.b == kNoQubit) bb = 1;
+                if (sa < 0 && sb < 0) {
+                    if (ba & bb) {
+                        if constexpr (PEND) {
+                            pend = cmul(pend, ph);
+                            pending = true;
+                        } else {
+                            scale_regs(v, w, ph);
+                        }
+                    }
+                    break;
                 }
-            break;
+                if (sa >= 0 && sb >= 0) {
+                    switch (sa * 8 + sb) {
+#define QK_P2(A, B)                                            \
+    case A * 8 + B:                                            \
+    case B * 8 + A:                                            \
+        reg_phase2<A, B>(v, ph);                               \
+        if constexpr (NS == 2) reg_phase2<A, B>(w, ph);        \
+        break;
+                    QK_P2(0, 1) QK_P2(0, 2) QK_P2(0, 3) QK_P2(0, 4) QK_P2(1, 2)
+                    QK_P2(1, 3) QK_P2(1, 4) QK_P2(2, 3) QK_P2(2, 4) QK_P2(3, 4)
+#undef QK_P2
+                    }
+                    break;
+                }
+                if (!(sa >= 0 ? bb : ba)) break;
+                switch (sa >= 0 ? sa : sb) {
+#define QK_P1(S)                                       \
+    case S:                                            \
+        reg_phase1<S>(v, ph);                          \
+        if constexpr (NS == 2) reg_phase1<S>(w, ph);   \
+        break;
+                QK_P1(0) QK_P1(1) QK_P1(2) QK_P1(3) QK_P1(4)
+#undef QK_P1
+                }
+                break;
+            }
         }
         case TOP_GRAD: {
             if constexpr (NS == 2) {
+                if constexpr (PEND) {
+                    if (pending) {
+                        scale_regs(v, w, pend);
+                        pend.x = 1;
+                        pend.y = 0;
+                        pending = false;
+                    }
+                }
                 // summed over the warp in the state's precision, added to
                 // the CTA's double accumulator once per warp
                 decltype(v[0].x) g = 0, g2 = 0;
@@ -541,6 +717,9 @@ __device__ __forceinline__ void run_program(C *tl, C *tw, uint64_t base, const P
         }
     }
     if (mapped) {
+        if constexpr (PEND) {
+            if (pending) scale_regs(v, w, pend);
+        }
 #pragma unroll
         for (int kk = 0; kk < R; ++kk) {
             const uint32_t x = reg_sidx<LOG2R>(kk, stb, sb);

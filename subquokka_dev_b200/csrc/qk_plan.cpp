@@ -22,6 +22,7 @@
 // can run the tile is re-distributed through shared memory (TOP_REMAP) so that
 // the qubits of the next ready gates become register bits.
 #include <algorithm>
+#include <complex>
 #include <array>
 #include <cstdint>
 #include <cstring>
@@ -106,6 +107,13 @@ struct PassBuilder {
     // tile bits of a pass: false, as the ops in order need them; true, grown
     // ahead by the qubit that lets the most pending ops join
     bool lookahead = false;
+    // diagonal ops with a qubit in a register slot wait for a re-mapping that
+    // takes it out (there they cost one multiply a thread, in a slot one
+    // for half or all of the thread's amplitudes), unless the op after them
+    // on one of their qubits could run now
+    bool defer_diagonals = false;
+    // no TOP_R1 / TOP_R2 and no pass marked xops
+    bool plain_ops = false;
 
     // Emit a pass over tile bits B running ops[idx] (in order, dependencies
     // already satisfied with respect to everything outside idx).
@@ -138,8 +146,28 @@ struct PassBuilder {
         };
         std::vector<int> Q;  // register slot -> tile-local bit
         auto in_regs = [&](int lq) { return std::find(Q.begin(), Q.end(), lq) != Q.end(); };
+        auto runnable = [&](const Op &op) {
+            bool ok = true;
+            for (int k = op_reg_first(op); k < op_reg_first(op) + op_reg_count(op); ++k)
+                ok = ok && in_regs(local[op.q[k]]);
+            return ok;
+        };
+        auto in_slot = [&](const Op &op) {
+            for (int k = 0; k < op.nq; ++k)
+                if (local[op.q[k]] >= 0 && in_regs(local[op.q[k]])) return true;
+            return false;
+        };
+        auto unblocks = [&](size_t i) {
+            const Op &op = ops[idx[i]];
+            for (int k = 0; k < op.nq; ++k) {
+                const std::vector<int> &qq = queue[op.q[k]];
+                const size_t h = head[op.q[k]] + 1;
+                if (h < qq.size() && !op_is_diagonal(ops[idx[qq[h]]]) && runnable(ops[idx[qq[h]]])) return true;
+            }
+            return false;
+        };
         size_t ndone = 0;
-        bool mapped = false;
+        bool mapped = false, flush = false;
         size_t done_at_remap = (size_t)-1;
         while (ndone < idx.size()) {
             bool progress = true;
@@ -149,10 +177,8 @@ struct PassBuilder {
                     if (done[i] || !ready(i)) continue;
                     const Op &op = ops[idx[i]];
                     if (!mapped) continue;  // the first program op is always a TOP_REMAP
-                    bool ok = true;
-                    for (int k = op_reg_first(op); k < op_reg_first(op) + op_reg_count(op); ++k)
-                        ok = ok && in_regs(local[op.q[k]]);
-                    if (!ok) continue;
+                    if (!runnable(op)) continue;
+                    if (defer_diagonals && !flush && op_is_diagonal(op) && in_slot(op) && !unblocks(i)) continue;
                     emit(op, local, Q);
                     done[i] = 1;
                     ++ndone;
@@ -161,6 +187,17 @@ struct PassBuilder {
                 }
             }
             if (ndone == idx.size()) break;
+            if (defer_diagonals && !flush && mapped) {
+                // waiting diagonal ops run now when only diagonal ops are
+                // left or the last re-mapping ran nothing
+                bool other = false;
+                for (size_t i = 0; i < idx.size() && !other; ++i) other = !done[i] && !op_is_diagonal(ops[idx[i]]);
+                if (!other || ndone == done_at_remap) {
+                    flush = true;
+                    continue;
+                }
+            }
+            flush = false;
             if (mapped && ndone == done_at_remap)
                 return fail(QK_ERR_ARG, "planner: a gate cannot be made register-resident (reg_bits %d)", r);
             done_at_remap = ndone;
@@ -195,6 +232,10 @@ struct PassBuilder {
         }
         d.nprog = (int)plan.ops.size() - d.prog0;
         d.ncoef = (int)(plan.coef.size() / 2) - d.coef0;
+        for (int i = d.prog0; i < d.prog0 + d.nprog && !plain_ops; ++i) {
+            const int k = plan.ops[i].kind;
+            d.xops |= k == TOP_R1 || k == TOP_R2 || k == TOP_DIAG || k == TOP_PHASE;
+        }
         d.ngrad = (int)plan.grad_params.size() - d.grad0;
         // program coefficient indices relative to the pass's slice
         for (int i = d.prog0; i < d.prog0 + d.nprog; ++i)
@@ -215,8 +256,14 @@ struct PassBuilder {
         auto slot = [&](int q) { return (int)(std::find(Q.begin(), Q.end(), local[q]) - Q.begin()); };
         switch (op.kind) {
         case OP_DENSE1:
-            t.kind = TOP_G1;
             t.a = (uint8_t)slot(op.q[0]);
+            if (!plain_ops && op_is_real(op)) {
+                t.kind = TOP_R1;
+                push_c(plan, op.m[0], op.m[2]);
+                push_c(plan, op.m[4], op.m[6]);
+                break;
+            }
+            t.kind = TOP_G1;
             for (int k = 0; k < 4; ++k) push_c(plan, op.m[2 * k], op.m[2 * k + 1]);
             break;
         case OP_GRAD: {
@@ -256,22 +303,19 @@ struct PassBuilder {
                 for (int i = 0; i < 4; ++i) m[2 * (4 * perm[i] + i)] = 1.0;
             }
             int sa = slot(op.q[0]), sb = slot(op.q[1]);
-            t.kind = TOP_G2;
-            if (sa < sb) {
-                t.a = (uint8_t)sa;
-                t.b = (uint8_t)sb;
-                for (int k = 0; k < 16; ++k) push_c(plan, m[2 * k], m[2 * k + 1]);
-            } else {
-                // index bit 0 must be the lower slot: swap the two index bits
-                t.a = (uint8_t)sb;
-                t.b = (uint8_t)sa;
-                auto sw = [](int i) { return ((i & 1) << 1) | ((i >> 1) & 1); };
-                for (int i = 0; i < 4; ++i)
-                    for (int j = 0; j < 4; ++j) {
-                        const int k = 4 * sw(i) + sw(j);
-                        push_c(plan, m[2 * k], m[2 * k + 1]);
-                    }
-            }
+            bool real = !plain_ops;
+            for (int k = 0; k < 16; ++k) real = real && m[2 * k + 1] == 0.0;
+            t.kind = real ? TOP_R2 : TOP_G2;
+            // index bit 0 must be the lower slot: swap the two index bits
+            auto sw = [&](int i) { return sa < sb ? i : ((i & 1) << 1) | ((i >> 1) & 1); };
+            t.a = (uint8_t)std::min(sa, sb);
+            t.b = (uint8_t)std::max(sa, sb);
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; j += real ? 2 : 1) {
+                    const int k = 4 * sw(i) + sw(j);
+                    if (real) push_c(plan, m[2 * k], m[2 * (4 * sw(i) + sw(j + 1))]);
+                    else push_c(plan, m[2 * k], m[2 * k + 1]);
+                }
             break;
         }
         case OP_CX:
@@ -559,7 +603,10 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
         std::vector<Op> ops = lowered;
         relabel_perms(ops, n, pass_low_bits(o, n), perm_tile_bits(o.dtype), 6, variant >= 4);
         merge_one_qubit_runs(ops, n);
-        absorb_into_two_qubit_ops(ops, n);
+        // real one-qubit ops stay real (TOP_R1 / TOP_R2 take half the
+        // multiply-adds of complex ones): the 30-qubit QFT 228 -> 219 ms
+        // complex128, 166 -> 163 ms complex64
+        absorb_into_two_qubit_ops(ops, n, !o.plain_ops);
         if (variant % 2) asap_order(ops, n);
         HostPlan hp;
         hp.n = n;
@@ -568,6 +615,12 @@ int build_plan(const qk_gate *gates, size_t ng, int n, const PlanOptions &o, Hos
         hp.r = o.reg_bits;
         PassBuilder b{ops, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), hp};
         b.lookahead = (variant >> 1) & 1;
+        // diagonal ops wait for their qubits to leave the register slots
+        // where the kernel carries a pending scalar (the 30-qubit QFT 163 ->
+        // 159 ms complex64; complex128 with 16 register amplitudes keeps
+        // none, and the extra re-mappings cost 219 -> 224 ms)
+        b.plain_ops = o.plain_ops != 0;
+        b.defer_diagonals = !o.plain_ops && pending_scalar_ok(o.dtype == QK_C128 ? 16 : 8, 1 << o.reg_bits, 1);
         rc = b.greedy(0, ops.size());
         if (rc) return rc;
         if (variant == 0 || hp.passes.size() < plan.passes.size() ||
@@ -644,6 +697,7 @@ int build_adjoint_plan(const qk_gate *gates, size_t ng, const int32_t *pidx, int
         hp.nstates = 2;
         PassBuilder b{list, n, o.tile_bits, o.reg_bits, pass_low_bits(o, n), hp};
         b.lookahead = variant >= 2;
+        b.plain_ops = o.plain_ops != 0;
         rc = b.greedy(0, list.size());
         if (rc) return rc;
         if (variant == 0 || hp.passes.size() < plan.passes.size() ||

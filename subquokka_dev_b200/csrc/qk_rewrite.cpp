@@ -102,6 +102,16 @@ void merge_one_qubit_runs(std::vector<Op> &ops, int n) {
     ops.swap(out);
 }
 
+// Real dense ops: a real 2 x 2 costs four multiply-adds an amplitude, a
+// complex one eight.
+bool op_is_real(const Op &op) {
+    const int nc = op.kind == OP_DENSE1 ? 4 : (op.kind == OP_DENSE2 || op.kind == OP_CDENSE1) ? 16 : 0;
+    if (!nc) return false;
+    for (int k = 0; k < nc; ++k)
+        if (op.m[2 * k + 1] != 0.0) return false;
+    return true;
+}
+
 // 4 x 4 matrix of a two-qubit op, index b(q[0]) + 2 b(q[1]), row-major (re, im).
 static void op_matrix4(const Op &op, double (&m)[32]) {
     std::memset(m, 0, sizeof m);
@@ -134,7 +144,12 @@ static void op_matrix4(const Op &op, double (&m)[32]) {
 // 30-qubit 20-layer circuit has 407 program ops instead of 941 and, though a
 // dense op needs both qubits in the tile (39 passes instead of 26), runs in
 // 679 ms instead of 725 ms (c128).
-void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n) {
+//
+// keep_real: no fold turns real one-qubit ops complex (the passes apply a
+// real 2 x 2 or 4 x 4 with half the multiply-adds of a complex one).  Two real pending ops before a complex two-qubit op become one
+// real 4 x 4 op (their tensor product) followed by that op; a real pending
+// op is not folded into a complex conditioned op.
+void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n, bool keep_real) {
     std::vector<long> last(n, -1);
     std::vector<char> dead;
     std::vector<Op> out;
@@ -177,11 +192,13 @@ void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n) {
                     mat2_mul(blk, um, res);
                     for (int k = 0; k < 8; ++k) f.m[8 * bc + k] = res[k];
                 }
-                dead[last[op.q[x]]] = 1;
-                last[op.q[0]] = last[op.q[1]] = -1;
-                out.push_back(f);
-                dead.push_back(0);
-                continue;
+                if (!(keep_real && op_is_real(u) && !op_is_real(f))) {
+                    dead[last[op.q[x]]] = 1;
+                    last[op.q[0]] = last[op.q[1]] = -1;
+                    out.push_back(f);
+                    dead.push_back(0);
+                    continue;
+                }
             }
         }
         if (two && last[op.q[0]] >= 0 && last[op.q[1]] >= 0) {
@@ -226,6 +243,17 @@ void absorb_into_two_qubit_ops(std::vector<Op> &ops, int n) {
                 } else {
                     f.kind = OP_DENSE2;
                     std::memcpy(f.m, m4, sizeof m4);
+                }
+                if (keep_real && dense && op_is_real(u0) && op_is_real(u1) && !op_is_real(f)) {
+                    // the real product of the two, then the op itself
+                    std::memcpy(f.m, k4, sizeof k4);
+                    dead[last[op.q[0]]] = dead[last[op.q[1]]] = 1;
+                    last[op.q[0]] = last[op.q[1]] = -1;
+                    out.push_back(f);
+                    dead.push_back(0);
+                    out.push_back(op);
+                    dead.push_back(0);
+                    continue;
                 }
                 dead[last[op.q[0]]] = dead[last[op.q[1]]] = 1;
                 last[op.q[0]] = last[op.q[1]] = -1;

@@ -185,6 +185,16 @@ void emulate(const HostPlan &hp, State &psi, State *lam, std::vector<double> &g)
                                 x[si][j1] = coef(op, off + 2) * a + coef(op, off + 3) * b;
                             });
                     break;
+                case qk::TOP_R1:
+                    for (int si = 0; si < 2; ++si)
+                        if (states[si])
+                            pairs(Q.at(op.a), [&](uint64_t j0, uint64_t j1) {
+                                const cd a = x[si][j0], b = x[si][j1];
+                                x[si][j0] = coef(op, 0).real() * a + coef(op, 0).imag() * b;
+                                x[si][j1] = coef(op, 1).real() * a + coef(op, 1).imag() * b;
+                            });
+                    break;
+                case qk::TOP_R2:
                 case qk::TOP_G2: {
                     const int ta = Q.at(op.a), tb = Q.at(op.b);
                     for (int si = 0; si < 2; ++si)
@@ -197,7 +207,11 @@ void emulate(const HostPlan &hp, State &psi, State *lam, std::vector<double> &g)
                                 for (int k = 0; k < 4; ++k) in[k] = x[si][idx[k]];
                                 for (int r = 0; r < 4; ++r) {
                                     out[r] = 0;
-                                    for (int k = 0; k < 4; ++k) out[r] += coef(op, 4 * r + k) * in[k];
+                                    for (int k = 0; k < 4; ++k) {
+                                        const cd c = coef(op, op.kind == qk::TOP_R2 ? 2 * r + k / 2 : 4 * r + k);
+                                        const double re = k % 2 ? c.imag() : c.real();
+                                        out[r] += op.kind == qk::TOP_R2 ? cd(re) * in[k] : c * in[k];
+                                    }
                                 }
                                 for (int k = 0; k < 4; ++k) x[si][idx[k]] = out[k];
                             }
@@ -274,14 +288,8 @@ int main() {
                 gates.push_back(G.gate());
             }
         }
-        HostPlan hp;
-        if (qk::build_plan(gates.data(), gates.size(), n, o, hp)) {
-            std::printf("seed %d: build_plan failed: %s\n", seed, qk_last_error());
-            ++bad;
-            continue;
-        }
-        ++plans;
-        State ref = G.state(), got = ref, dummy = ref;
+        const State init = G.state();
+        State ref = init;
         std::vector<double> none(1, 0);
         for (const qk_gate &g : gates) {
             std::vector<int> qs;
@@ -289,13 +297,29 @@ int main() {
             const auto m = matrix_of(op, qs);
             apply_matrix(ref, n, qs, m);
         }
-        emulate(hp, got, nullptr, none);
-        const double df = max_diff(ref, got);
-        if (df > 1e-12) {
-            std::printf("forward seed %d (n %d, T %d, r %d): max |d amp| %.3g, %zu passes\n", seed, n, T, r, df,
-                        hp.passes.size());
-            ++bad;
+        // default programs (real ops, deferred diagonal ops) and those of
+        // the batched kernel (plain ops)
+        bool failed = false;
+        for (int plain : {0, 1}) {
+            o.plain_ops = plain;
+            HostPlan hp;
+            if (qk::build_plan(gates.data(), gates.size(), n, o, hp)) {
+                std::printf("seed %d: build_plan failed: %s\n", seed, qk_last_error());
+                ++bad;
+                failed = true;
+                break;
+            }
+            ++plans;
+            State got = init;
+            emulate(hp, got, nullptr, none);
+            const double df = max_diff(ref, got);
+            if (df > 1e-12) {
+                std::printf("forward seed %d plain %d (n %d, T %d, r %d): max |d amp| %.3g, %zu passes\n", seed, plain,
+                            n, T, r, df, hp.passes.size());
+                ++bad;
+            }
         }
+        if (failed) continue;
         // tensor-core dense blocks (64 x 64 unitaries on six qubits, block
         // index bit b = qubit q[b]; permutation blocks for the restore)
         // (both dtypes: their permutation blocks have different tile limits)
@@ -344,7 +368,7 @@ int main() {
             const bool rot = g.kind == QK_GATE_RX || g.kind == QK_GATE_RY || g.kind == QK_GATE_RZ;
             pidx.push_back(rot ? (np > 2 && G.rng() % 4 == 0 ? (int)(G.rng() % np) : np++) : -1);
         }
-        qk::PlanOptions ao{o.dtype, std::min(T, 6), 2 + seed % 2};
+        qk::PlanOptions ao{o.dtype, std::min(T, 6), 2 + seed % 2, seed % 5 == 0};
         HostPlan ap;
         if (qk::build_adjoint_plan(circ.data(), circ.size(), pidx.data(), n, ao, ap)) {
             std::printf("seed %d: build_adjoint_plan failed: %s\n", seed, qk_last_error());
