@@ -52,13 +52,7 @@ __global__ void __launch_bounds__(NARROW ? 128 : pass_max_threads<C, R, NS>(), N
         for (int i = threadIdx.x; i < d.ngrad; i += NT) gsm[i] = 0.0;
     if (d.perm) {
         // permutation pass: plain load / permuted store, one buffer
-        for (uint64_t o = blockIdx.x; o < ntiles; o += gridDim.x) {
-            const uint64_t base = pass_base(o, d);
-            for (uint32_t j = threadIdx.x; j < N; j += NT) buf0[swz<C>(j)] = s[base | pass_off(j, d)];
-            __syncthreads();
-            run_perm_tile(s, buf0, base, d, N, NT);
-            __syncthreads();
-        }
+        run_perm_pass(s, buf0, ntiles, d, N, NT);
         return;
     }
     TileAddr<C, LOG2R> ta;

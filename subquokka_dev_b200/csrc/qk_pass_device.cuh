@@ -286,16 +286,64 @@ __device__ __forceinline__ void prefetch_tile(C *buf, const C *__restrict__ s, u
     cp_async_commit();
 }
 
-// Permutation pass: tile element j goes to the position of perm(j).
+// Tile-local image of j under a permutation pass's bit-pair swaps.
+__device__ __forceinline__ uint32_t perm_bits(uint32_t j, const PassDesc &d) {
+    uint32_t f = j;
+    for (int i = 0; i < d.nperm; ++i) {
+        const uint32_t a = (j >> d.perm_a[i]) & 1, b = (j >> d.perm_b[i]) & 1;
+        f = (f & ~(1u << d.perm_a[i]) & ~(1u << d.perm_b[i])) | (b << d.perm_a[i]) | (a << d.perm_b[i]);
+    }
+    return f;
+}
+
+// Permutation pass: tile element j goes to the position of perm(j).  A
+// thread moves the elements j = tid + i NT (i < N / NT <= 32).  The load
+// offset (a bit deposit), the store offset (a bit permutation, then the
+// deposit) and the shared-memory index (an XOR fold) are each linear in j
+// over disjoint bits, so each is the thread's part combined with the parts
+// of the set bits of i, computed once per thread: the per-element work is a
+// few ORs instead of a loop over the tile bits.
 template <typename C>
-__device__ void run_perm_tile(C *__restrict__ s, C *tl, uint64_t base, const PassDesc &d, uint32_t N, uint32_t NT) {
-    for (uint32_t j = threadIdx.x; j < N; j += NT) {
-        uint32_t f = j;
-        for (int i = 0; i < d.nperm; ++i) {
-            const uint32_t a = (j >> d.perm_a[i]) & 1, b = (j >> d.perm_b[i]) & 1;
-            f = (f & ~(1u << d.perm_a[i]) & ~(1u << d.perm_b[i])) | (b << d.perm_a[i]) | (a << d.perm_b[i]);
+__device__ void run_perm_pass(C *__restrict__ s, C *buf, uint64_t ntiles, const PassDesc &d, uint32_t N,
+                              uint32_t NT) {
+    constexpr int kMaxB = 5;
+    const uint32_t tid = threadIdx.x;
+    const uint64_t ld_t = pass_off(tid, d), st_t = pass_off(perm_bits(tid, d), d);
+    const uint32_t sw_t = swz<C>(tid);
+    uint64_t ld_u[kMaxB], st_u[kMaxB];
+    uint32_t sw_u[kMaxB];
+    int nb = 0;
+#pragma unroll
+    for (int b = 0; b < kMaxB; ++b) {
+        const uint32_t m = NT << b;
+        ld_u[b] = m < N ? pass_off(m, d) : 0;
+        st_u[b] = m < N ? pass_off(perm_bits(m, d), d) : 0;
+        sw_u[b] = m < N ? swz<C>(m) : 0;
+        nb += m < N;
+    }
+    const uint32_t R = 1u << nb;
+    for (uint64_t o = blockIdx.x; o < ntiles; o += gridDim.x) {
+        const uint64_t base = pass_base(o, d);
+        for (uint32_t i = 0; i < R; ++i) {
+            uint64_t a = ld_t;
+            uint32_t x = sw_t;
+#pragma unroll
+            for (int b = 0; b < kMaxB; ++b)
+                if ((i >> b) & 1) { a |= ld_u[b]; x ^= sw_u[b]; }
+            cp_async_amp(buf + x, s + (base | a));
         }
-        s[base | pass_off(f, d)] = tl[swz<C>(j)];
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        for (uint32_t i = 0; i < R; ++i) {
+            uint64_t a = st_t;
+            uint32_t x = sw_t;
+#pragma unroll
+            for (int b = 0; b < kMaxB; ++b)
+                if ((i >> b) & 1) { a |= st_u[b]; x ^= sw_u[b]; }
+            s[base | a] = buf[x];
+        }
+        __syncthreads();
     }
 }
 
