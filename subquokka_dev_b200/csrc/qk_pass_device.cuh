@@ -296,51 +296,53 @@ __device__ __forceinline__ uint32_t perm_bits(uint32_t j, const PassDesc &d) {
     return f;
 }
 
-// Permutation pass: tile element j goes to the position of perm(j).  A
-// thread moves the elements j = tid + i NT (i < N / NT <= 32).  The load
-// offset (a bit deposit), the store offset (a bit permutation, then the
-// deposit) and the shared-memory index (an XOR fold) are each linear in j
+// Permutation pass: tile element j goes to the position of perm(j) (perm
+// is a product of disjoint bit-pair swaps, its own inverse).  A thread
+// loads the elements f = tid + i NT (i < N / NT <= 32) and stores, at the
+// same positions, the elements perm(f), read from the shared-memory tile:
+// both global accesses stay in the tile's contiguous runs, the permutation
+// is a shared-memory gather.  The state offset (a bit deposit) and the
+// shared-memory indices of f and perm(f) (an XOR fold) are each linear in f
 // over disjoint bits, so each is the thread's part combined with the parts
-// of the set bits of i, computed once per thread: the per-element work is a
-// few ORs instead of a loop over the tile bits.
+// of the set bits of i, computed once per thread.
 template <typename C>
 __device__ void run_perm_pass(C *__restrict__ s, C *buf, uint64_t ntiles, const PassDesc &d, uint32_t N,
                               uint32_t NT) {
     constexpr int kMaxB = 5;
     const uint32_t tid = threadIdx.x;
-    const uint64_t ld_t = pass_off(tid, d), st_t = pass_off(perm_bits(tid, d), d);
-    const uint32_t sw_t = swz<C>(tid);
-    uint64_t ld_u[kMaxB], st_u[kMaxB];
-    uint32_t sw_u[kMaxB];
+    const uint64_t g_t = pass_off(tid, d);
+    const uint32_t sw_t = swz<C>(tid), sp_t = swz<C>(perm_bits(tid, d));
+    uint64_t g_u[kMaxB];
+    uint32_t sw_u[kMaxB], sp_u[kMaxB];
     int nb = 0;
 #pragma unroll
     for (int b = 0; b < kMaxB; ++b) {
         const uint32_t m = NT << b;
-        ld_u[b] = m < N ? pass_off(m, d) : 0;
-        st_u[b] = m < N ? pass_off(perm_bits(m, d), d) : 0;
+        g_u[b] = m < N ? pass_off(m, d) : 0;
         sw_u[b] = m < N ? swz<C>(m) : 0;
+        sp_u[b] = m < N ? swz<C>(perm_bits(m, d)) : 0;
         nb += m < N;
     }
     const uint32_t R = 1u << nb;
     for (uint64_t o = blockIdx.x; o < ntiles; o += gridDim.x) {
         const uint64_t base = pass_base(o, d);
         for (uint32_t i = 0; i < R; ++i) {
-            uint64_t a = ld_t;
+            uint64_t a = g_t;
             uint32_t x = sw_t;
 #pragma unroll
             for (int b = 0; b < kMaxB; ++b)
-                if ((i >> b) & 1) { a |= ld_u[b]; x ^= sw_u[b]; }
+                if ((i >> b) & 1) { a |= g_u[b]; x ^= sw_u[b]; }
             cp_async_amp(buf + x, s + (base | a));
         }
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
         for (uint32_t i = 0; i < R; ++i) {
-            uint64_t a = st_t;
-            uint32_t x = sw_t;
+            uint64_t a = g_t;
+            uint32_t x = sp_t;
 #pragma unroll
             for (int b = 0; b < kMaxB; ++b)
-                if ((i >> b) & 1) { a |= st_u[b]; x ^= sw_u[b]; }
+                if ((i >> b) & 1) { a |= g_u[b]; x ^= sp_u[b]; }
             s[base | a] = buf[x];
         }
         __syncthreads();
