@@ -4,8 +4,10 @@
 // U2 matrices, CNOT-shaped U2s, VSWAPs) are run on small dense states by an
 // independent simulator below, once as generated and once after the
 // rewrites the planners apply:
-// - forward lists: merge_one_qubit_runs, absorb_into_two_qubit_ops,
-//   asap_order, relabel_perms; the final states must agree;
+// - forward lists: merge_one_qubit_runs, absorb_into_two_qubit_ops (with
+//   and without keep_real, which leaves real one-qubit ops real and may
+//   emit a real 4 x 4 op before a complex two-qubit op), asap_order,
+//   relabel_perms; the final states must agree;
 // - backward lists with gradient ops (Im <lambda|G|psi>, G = X, Y, Z):
 //   hoist_gradients, merge_one_qubit_runs, absorb_into_two_qubit_ops,
 //   pair_gradients; the final states and every gradient must agree.
@@ -32,7 +34,8 @@ int main() {
         std::vector<Op> rw = ops;
         qk::relabel_perms(rw, n, 2, 8, 2, seed % 2 == 0);
         qk::merge_one_qubit_runs(rw, n);
-        qk::absorb_into_two_qubit_ops(rw, n);
+        const bool keep_real = seed % 4 >= 2;
+        qk::absorb_into_two_qubit_ops(rw, n, keep_real);
         if (seed % 2) qk::asap_order(rw, n);
         State p0 = G.state(), l0 = p0, p1 = p0, l1 = p0;
         std::vector<double> g0(64, 0), g1(64, 0);
@@ -40,7 +43,8 @@ int main() {
         run(rw, n, p1, l1, g1);
         const double df = max_diff(p0, p1);
         if (df > 1e-12) {
-            std::printf("forward seed %d: max |d amp| %.3g (%zu -> %zu ops)\n", seed, df, ops.size(), rw.size());
+            std::printf("forward seed %d (keep_real %d): max |d amp| %.3g (%zu -> %zu ops)\n", seed, (int)keep_real, df,
+                        ops.size(), rw.size());
             ++bad;
         }
         // backward list: gradient ops on random qubits between the ops
